@@ -1,0 +1,335 @@
+"""Benchmark: all-pairs Needleman-Wunsch GCUPS on one B200 (or N, weak scaling).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--workload c3|c2|c4]
+    python bench.py --impl reference ...      # the reference's CPU path
+
+A step is one all-pairs scoring pass over the workload (c3 by default: 4,000
+uneven DNA sequences, ~8.0M pairs). `value` is kernel-resident throughput
+(inputs already in HBM); `e2e` goes through the public C ABI with host buffers
+(sequence upload and score download inside the timed region). GCUPS counts
+sum over pairs of L_i * L_j with unpadded lengths.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "all-pairs NW GCUPS (bit-exact) batched vs plain"
+
+
+def _rank_info():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines: list[str] = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for k, name in enumerate(names):
+                if parts[5 + k].lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def load_workload(name: str, rank: int = 0):
+    from msa_b200 import workloads as W
+    if name == "c3":
+        return W.c3(seed=3 + 1000 * rank)
+    if name == "c2":
+        return W.c2(seed=2 + 1000 * rank)
+    if name == "c4":
+        return W.c4(seed=4 + 1000 * rank)
+    raise SystemExit(f"unknown workload {name}")
+
+
+def workload_config(name: str, wl) -> dict:
+    L = wl.lengths()
+    cfg = {"workload": {"c3": "4000 uneven DNA (log-normal median 1500, sigma 0.75, clip [200,16000]), default +1/-1 table, gap 1",
+                        "c2": "1000 proteins from a 500-aa ancestor (subst U[0.10,0.30], indel 0.02), blosum62, gap 4",
+                        "c4": "2000 proteins, 20 clades of 100, lengths U[200,1200], blosum62, gap 4"}[name],
+           "sequences": wl.n, "pairs": wl.n * (wl.n - 1) // 2, "cells": wl.cells(),
+           "mean_len": float(L.mean()), "max_len": int(L.max()), "table": wl.table, "seed": wl.seed}
+    return cfg
+
+
+# ---------------------------------------------------------------- CPU reference arm
+
+def cpu_reference_sample(wl, target_cells: float, seed: int = 77):
+    """A seeded uniform sample of the workload's pairs holding ~target_cells cells."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    L = wl.lengths().astype(np.float64)
+    n = wl.n
+    mean_cells = (L.sum() ** 2 - (L * L).sum()) / (n * (n - 1))
+    k = max(8, int(target_cells / mean_cells))
+    i = rng.integers(1, n, k)
+    j = (rng.random(k) * i).astype(np.int64)
+    cells = float((L[i] * L[j]).sum())
+    return i.astype(np.int32), j.astype(np.int32), cells
+
+
+def run_cpu_reference(wl, steps: int, warmup: int, target_cells: float):
+    from oracle import oracle as O
+    if O.reference() is None:
+        return None
+    threads = os.cpu_count() or 1
+    strings = wl.strings()
+    times, cells_all = [], []
+    for s in range(warmup + steps):
+        i, j, cells = cpu_reference_sample(wl, target_cells, seed=77 + s)
+        t0 = time.perf_counter()
+        O.ref_nw_pairs(strings, i, j, wl.table, threads=threads)
+        dt = time.perf_counter() - t0
+        if s >= warmup:
+            times.append(dt)
+            cells_all.append(cells)
+    gcups = sum(cells_all) / sum(times) / 1e9
+    return {"value": gcups, "unit": "GCUPS", "cores": threads, "kind": "reference",
+            "sample": f"{len(times)} x ~{target_cells:.2g}-cell uniform pair samples of the workload, "
+                      f"Museqa needleman::sequential (oracle/_ref) on {threads} host threads",
+            "seconds": sum(times)}
+
+
+def reference_arm(args):
+    rank, world, _ = _rank_info()
+    if rank != 0:
+        return
+    wl = load_workload(args.workload)
+    res = run_cpu_reference(wl, args.steps, args.warmup, args.cpu_cells)
+    if res is None:
+        print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref/libmuseqa_ref.so was not built"}))
+        return
+    line = {"metric": METRIC, "value": res["value"], "unit": "GCUPS", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1000.0 * res["seconds"] / max(args.steps, 1),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded)", "config": workload_config(args.workload, wl), "impl": "reference",
+            "cpu_baseline": res, "e2e": {"value": res["value"], "unit": "GCUPS", "h2d_bytes_per_step": 0,
+                                         "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+# ---------------------------------------------------------------- GPU arm
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="c3", choices=["c3", "c2", "c4"])
+    ap.add_argument("--plain-steps", type=int, default=1)
+    ap.add_argument("--cpu-cells", type=float, default=1.5e10)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+
+    import ctypes
+
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = _rank_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=600))
+
+    from msa_b200 import ScoringTable, _lib, runtime
+    lib = _lib.lib()
+    ctx = runtime.context(local)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+
+    wl = load_workload(args.workload, rank)
+    cfg = workload_config(args.workload, wl)
+    table = ScoringTable(wl.table)
+    flat, offs, lens = wl.flat_units()
+    n = wl.n
+    npairs = n * (n - 1) // 2
+    u8, u64 = ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint64)
+
+    h = ctypes.c_uint64()
+    _lib.check(lib.msa_seqs_upload(ctx.handle, flat.ctypes.data_as(u8), offs.ctypes.data_as(u64),
+                                   lens.ctypes.data_as(u64), n, ctypes.byref(h)), ctx.handle)
+    out = torch.empty(npairs, dtype=torch.int32, device=f"cuda:{local}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")   # > 126 MB L2
+
+    def run(mode):
+        _lib.check(lib.msa_nw_all_pairs(ctx.handle, h.value, ctypes.byref(table._t), mode,
+                                        ctypes.c_void_p(out.data_ptr()), 1), ctx.handle)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def timed(mode, steps, warmup):
+        for _ in range(warmup):
+            run(mode)
+        barrier()
+        ms, kms = [], []
+        launches0 = ctx.launches
+        for _ in range(steps):
+            flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            run(mode)
+            e1.record(stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            st = _lib.MsaNwStats()
+            lib.msa_nw_last_stats(ctx.handle, ctypes.byref(st))
+            kms.append(st.kernel_ms)
+        barrier()
+        return ms, kms, ctx.launches - launches0, st
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms, kms, launches, st = timed(_lib.MSA_NW_PERSISTENT, args.steps, args.warmup)
+    clocks = sampler.stop()
+    plain_ms, plain_kms, _, _ = timed(_lib.MSA_NW_PLAIN, args.plain_steps, 1)
+
+    # Bit-exact cross-check of the two kernels on this workload.
+    run(_lib.MSA_NW_PERSISTENT)
+    a = out.clone()
+    run(_lib.MSA_NW_PLAIN)
+    agree = bool(torch.equal(a, out))
+
+    # End to end through the public C ABI: pinned host units in, host scores out.
+    pin_units = torch.from_numpy(flat).pin_memory()
+    host_out = torch.empty(npairs, dtype=torch.int32).pin_memory()
+    e2e_ms = []
+    for s in range(1 + args.steps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        barrier()
+        e0.record(stream)
+        h2 = ctypes.c_uint64()
+        _lib.check(lib.msa_seqs_upload(ctx.handle, ctypes.cast(pin_units.data_ptr(), u8), offs.ctypes.data_as(u64),
+                                       lens.ctypes.data_as(u64), n, ctypes.byref(h2)), ctx.handle)
+        _lib.check(lib.msa_nw_all_pairs(ctx.handle, h2.value, ctypes.byref(table._t), _lib.MSA_NW_PERSISTENT,
+                                        ctypes.c_void_p(host_out.data_ptr()), 0), ctx.handle)
+        e1.record(stream)
+        e1.synchronize()
+        lib.msa_seqs_release(ctx.handle, h2.value)
+        if s >= 1:
+            e2e_ms.append(e0.elapsed_time(e1))
+    e2e_ok = bool(torch.equal(host_out, a.cpu()))
+
+    # Max over ranks.
+    def maxr(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    step_ms = maxr(float(np.mean(ms)))
+    kern_ms = maxr(float(np.mean(kms)))
+    plain_step = maxr(float(np.mean(plain_ms)))
+    e2e_step = maxr(float(np.mean(e2e_ms)))
+    cells_all = cfg["cells"] * world
+    value = cells_all / (step_ms / 1e3) / 1e9
+    kernel_gcups = cfg["cells"] / (kern_ms / 1e3) / 1e9
+    plain_gcups = cells_all / (plain_step / 1e3) / 1e9
+    e2e_gcups = cells_all / (e2e_step / 1e3) / 1e9
+
+    if rank == 0:
+        props = torch.cuda.get_device_properties(local)
+        sm_mhz = clocks.get("sm_mhz") or 1965.0
+        # INT32 issue roofline: 4 SM sub-partitions x 32 lanes issue per clock;
+        # 4 algorithmic lane-ops per cell (d+s, max(up,left), -g, max).
+        peak = props.multi_processor_count * 128 * sm_mhz * 1e6 / 4 / 1e9
+        traffic = None
+        tp = ROOT / "profiles" / "nw_traffic.json"
+        if tp.exists():
+            try:
+                traffic = json.loads(tp.read_text()).get(args.workload)
+            except Exception:
+                traffic = None
+        cpu = None
+        if not args.no_cpu:
+            cpu = run_cpu_reference(wl, 1, 0, args.cpu_cells)
+        line = {
+            "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int32/int16x2", "data": "synthetic (seeded)",
+            "config": dict(cfg, parallelism=f"{world} independent replicas (weak)" if world > 1 else "1 GPU",
+                           l2="flushed (256 MB write) before every timed step"),
+            "kernel_gcups": kernel_gcups, "narrow_tasks": int(st.narrow_tasks),
+            "plain": {"value": plain_gcups, "ms_per_step": plain_step, "steps": args.plain_steps,
+                      "speedup_persistent_vs_plain": value / plain_gcups, "bit_identical": agree},
+            "e2e": {"value": e2e_gcups, "unit": "GCUPS", "ms_per_step": e2e_step,
+                    "h2d_bytes_per_step": int(flat.nbytes + offs.nbytes + lens.nbytes),
+                    "d2h_bytes_per_step": int(npairs * 4), "scores_match": e2e_ok},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "int32-issue", "achieved": kernel_gcups, "peak": peak, "unit": "GCUPS",
+                         "frac": kernel_gcups / peak, "traffic": traffic,
+                         "peak_basis": f"{props.multi_processor_count} SM x 128 lanes/clk x {sm_mhz:.0f} MHz "
+                                       f"(median sampled) / 4 INT32 ops per cell"},
+            "clocks": clocks,
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line))
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

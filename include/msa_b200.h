@@ -1,0 +1,195 @@
+/*
+ * msa_b200 — C ABI of the B200-native all-pairs Needleman-Wunsch and
+ * neighbor-joining library (libmsa_b200.so).
+ *
+ * Plain pointers and sizes only. Every entry point returns an msa_status;
+ * nothing throws across this boundary. A context owns one CUDA stream and
+ * the device buffers it allocates; use one context per host thread.
+ *
+ * Each declaration names the reference interface it replaces (Museqa
+ * v0.1.1, paths relative to the project root).
+ */
+#ifndef MSA_B200_H
+#define MSA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+
+typedef enum msa_status {
+    MSA_OK = 0,
+    MSA_ERR_INVALID = 1,            /* bad argument (null pointer, size, unit code) */
+    MSA_ERR_CUDA = 2,               /* a CUDA runtime call failed; see msa_last_error */
+    MSA_ERR_NOMEM = 3,              /* device or host allocation failed */
+    MSA_ERR_UNKNOWN_TABLE = 4,      /* "unknown pairwise scoring table '%s'" (src/pairwise/table.cu:315-321) */
+    MSA_ERR_UNKNOWN_ALGORITHM = 5,  /* "unknown pairwise/phylogeny algorithm '%s'" (src/pairwise/pairwise.cpp:298-303) */
+    MSA_ERR_HANDLE = 6,             /* stale or foreign sequence-store handle */
+    MSA_ERR_DEVICE_TIMEOUT = 7,     /* a bounded device-side wait gave up; the context stays usable */
+    MSA_ERR_UNDEFINED = 8,          /* input whose result the reference leaves undefined (see msa_nw_all_pairs) */
+    MSA_ERR_NO_DEVICE = 9,          /* no CUDA device, or the library was built without a usable kernel image */
+    MSA_ERR_QUEUE = 10,             /* serving queue closed, full, or job id unknown */
+    MSA_ERR_TOO_LARGE = 11          /* request exceeds a stated size limit */
+} msa_status;
+
+/* Message for a status code. */
+const char *msa_strerror(int status);
+
+/* ----------------------------------------------------------------- tables */
+
+/* Number of scoring-table entries per side; rows and columns are encoder units. */
+#define MSA_TABLE_SIDE 25
+
+/*
+ * A scoring table by value: scoring_table (src/pairwise/pairwise.cuh:124-182).
+ * `score[x*25+y]` is the score of units x and y; `penalty` is the positive
+ * linear gap penalty that is subtracted. `index` is the table's position in
+ * the built-in storage order (default, blosum62, blosum45, blosum50,
+ * blosum80, blosum90, pam250; src/pairwise/table.cu:41-262), or -1 for a
+ * caller-made table.
+ */
+typedef struct msa_table {
+    int32_t score[MSA_TABLE_SIDE * MSA_TABLE_SIDE];
+    int32_t penalty;
+    int32_t index;
+} msa_table;
+
+/* scoring_table::make(name) (src/pairwise/table.cu:315-321). */
+int msa_table_make(const char *name, msa_table *out);
+/* scoring_table::has(name) (src/pairwise/table.cu:305-308): 1 or 0. */
+int msa_table_has(const char *name);
+/* scoring_table::list() (src/pairwise/table.cu:327-330): names in the
+ * reference's (sorted) order. Returns the count; fills up to `cap` names. */
+int msa_table_list(const char **names, int cap);
+
+/* ---------------------------------------------------------------- encoder */
+
+/* Unit codes (src/encoder.hpp:42-48). */
+#define MSA_UNIT_END 0x18
+#define MSA_UNIT_GAP 0x19
+
+/* encoder::encode(char) (src/encoder.cpp:46-57) over `len` characters into
+ * one byte per unit. */
+int msa_encode(const char *chars, uint64_t len, uint8_t *out_units);
+/* encoder::decode(unit) (src/encoder.cpp:36-39, :62-66) into characters. */
+int msa_decode(const uint8_t *units, uint64_t len, char *out_chars);
+/* encoder::encode(const char*, size_t) (src/encoder.cpp:76-98): the
+ * reference's packed form, 3 units per uint16 block, bit 0 = padded block.
+ * Returns MSA_OK; ceil(len/3) blocks written. */
+int msa_encode_blocks(const char *chars, uint64_t len, uint16_t *out_blocks);
+/* Inverse of the packed form: 3*nblocks units. */
+int msa_unpack_blocks(const uint16_t *blocks, uint64_t nblocks, uint8_t *out_units);
+
+/* ---------------------------------------------------------------- context */
+
+typedef struct msa_ctx msa_ctx;
+
+/* Creates a context on `device` (the CLI's -d/--device, src/museqa.cpp:34). */
+int msa_create(int device, msa_ctx **out);
+void msa_destroy(msa_ctx *ctx);
+/* Detail of the context's last failure (empty if none). */
+const char *msa_last_error(const msa_ctx *ctx);
+/* Makes the context launch on `stream` (a cudaStream_t; NULL = the context's
+ * own stream). The caller keeps the stream alive while the context uses it. */
+int msa_set_stream(msa_ctx *ctx, void *stream);
+void *msa_get_stream(msa_ctx *ctx);
+/* Number of this library's kernel launches issued by the context so far. */
+uint64_t msa_launch_count(const msa_ctx *ctx);
+
+/* ---------------------------------------------------------- sequence store */
+
+typedef uint64_t msa_seqs;
+
+/*
+ * Uploads n sequences of encoder units into device memory: the device-resident
+ * replacement of pairwise::database (src/pairwise/database.cuh:27-91,
+ * src/pairwise/database.cu:24-72). Sequence k is units[offs[k] .. offs[k]+lens[k]).
+ * Units past lens[k] up to the next multiple of 3 are END, as in the
+ * reference's block padding (src/sequence.hpp:101-104). Unit codes must be
+ * 0..25. The caller's arrays may be freed after the call returns.
+ */
+int msa_seqs_upload(msa_ctx *ctx, const uint8_t *units, const uint64_t *offs,
+                    const uint64_t *lens, uint32_t n, msa_seqs *out);
+int msa_seqs_release(msa_ctx *ctx, msa_seqs seqs);
+/* Number of sequences in a store, or -1 for a bad handle. */
+int64_t msa_seqs_count(msa_ctx *ctx, msa_seqs seqs);
+
+/* ---------------------------------------------------------- all-pairs NW */
+
+typedef enum msa_nw_mode {
+    MSA_NW_AUTO = 0,        /* = MSA_NW_PERSISTENT */
+    MSA_NW_PLAIN = 1,       /* one launch per length bucket, one pair per warp, int32 */
+    MSA_NW_PERSISTENT = 2   /* one persistent work-stealing launch over cost-ordered tiles,
+                               autotuned tile shapes, 16-bit lanes where provably exact,
+                               replayed from a CUDA graph */
+} msa_nw_mode;
+
+/*
+ * Scores every pair i > j of the store with global linear-gap
+ * Needleman-Wunsch and writes out[i*(i-1)/2 + j] (int32): the scoring step of
+ * needleman::sequential / needleman::hybrid
+ * (src/pairwise/needleman/impl/sequential.cpp:29-122,
+ * src/pairwise/needleman/impl/hybrid.cu:403-456) with the packed
+ * lower-triangle layout of distance_matrix (src/pairwise/pairwise.cuh:53-117).
+ * Scores equal the reference's float scores exactly (they are small integers);
+ * the reference's treatment of END units inside a sequence (row truncation,
+ * column skipping) is reproduced.
+ *
+ * `out` is host memory (out_on_device = 0) or device memory of this context's
+ * device (out_on_device = 1). Returns MSA_ERR_UNDEFINED when a GAP unit (25)
+ * would index past the reference's table storage (pam250 or a caller table),
+ * which is undefined behaviour in the reference.
+ */
+int msa_nw_all_pairs(msa_ctx *ctx, msa_seqs seqs, const msa_table *table, int mode,
+                     int32_t *out, int out_on_device);
+
+/* Timing breakdown of the context's last msa_nw_all_pairs call (device ms). */
+typedef struct msa_nw_stats {
+    double kernel_ms;       /* NW kernels only */
+    double total_ms;        /* whole device-side call, profile build included */
+    uint64_t cells;         /* sum over pairs of (effective rows x effective columns) */
+    uint64_t pairs;
+    uint32_t launches;      /* kernel launches issued by the call */
+    uint32_t narrow_tasks;  /* tasks run on 16-bit lanes */
+} msa_nw_stats;
+int msa_nw_last_stats(const msa_ctx *ctx, msa_nw_stats *out);
+
+/* ---------------------------------------------------------- neighbor-joining */
+
+/* One node of the guide tree: otu + hierarchy
+ * (src/phylogeny/phylogeny.cuh:171-180, src/hierarchy.hpp:46-47).
+ * Undefined references are 0xFFFFFFFF. */
+typedef struct msa_otu {
+    uint32_t parent;
+    uint32_t child[2];
+    float distance;
+    uint32_t level;
+} msa_otu;
+
+typedef enum msa_tri_kind {
+    MSA_TRI_F32_HOST = 0,
+    MSA_TRI_F32_DEVICE = 1,
+    MSA_TRI_I32_HOST = 2,
+    MSA_TRI_I32_DEVICE = 3
+} msa_tri_kind;
+
+/*
+ * Neighbor-joining over the packed lower triangle `tri` (n(n-1)/2 values,
+ * index i(i-1)/2+j; int32 kinds are converted to float exactly): the
+ * replacement of njoining::sequential_symmetric / hybrid_symmetric
+ * (src/phylogeny/njoining/impl/sequential.cpp:80-346,
+ * src/phylogeny/njoining/impl/hybrid.cu:149-543). Writes 2n-1 nodes, leaves
+ * 0..n-1, parents n..2n-2 in join order, root 2n-2. The joins, branch lengths
+ * and levels equal the reference's sequential symmetric algorithm bit for bit.
+ * n < 2 writes nothing (phylogeny returns an empty tree).
+ */
+int msa_nj(msa_ctx *ctx, const void *tri, int tri_kind, uint32_t n, msa_otu *out_nodes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,347 @@
+// C ABI of libmsa_b200.so: contexts, the device-resident sequence store and
+// the all-pairs NW / NJ entry points. Every entry point catches everything
+// and returns a status; nothing throws across the boundary.
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <numeric>
+#include <string>
+
+#include "msa_internal.hpp"
+
+namespace msa {
+
+cudaError_t DevBuf::ensure(size_t need)
+{
+    if(need <= bytes && ptr) return cudaSuccess;
+    if(ptr) { cudaFree(ptr); ptr = nullptr; bytes = 0; }
+    size_t want = std::max<size_t>(need, 256);
+    cudaError_t e = cudaMalloc(&ptr, want);
+    if(e != cudaSuccess) { ptr = nullptr; bytes = 0; cudaGetLastError(); return e; }
+    bytes = want;
+    return cudaSuccess;
+}
+
+void DevBuf::release()
+{
+    if(ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+int set_error(msa_ctx *ctx, int status, const std::string &msg)
+{
+    if(ctx) ctx->err = msg;
+    return status;
+}
+
+int cuda_error(msa_ctx *ctx, cudaError_t e, const char *what)
+{
+    std::string m = std::string(what) + ": " + cudaGetErrorString(e);
+    cudaGetLastError();
+    return set_error(ctx, e == cudaErrorMemoryAllocation ? MSA_ERR_NOMEM : MSA_ERR_CUDA, m);
+}
+
+static void free_store(SeqStore *st)
+{
+    if(!st) return;
+    cudaFree(st->d_units);
+    cudaFree(st->d_off);
+    cudaFree(st->d_eff);
+    cudaFree(st->d_plen);
+    cudaFree(st->d_clean_sorted);
+    cudaFree(st->d_prof_off);
+    cudaFree(st->d_prof_lp);
+    delete st;
+}
+
+void release_graphs(msa_ctx *ctx);
+
+}  // namespace msa
+
+using namespace msa;
+
+extern "C" {
+
+int msa_create(int device, msa_ctx **out)
+{
+    if(!out) return MSA_ERR_INVALID;
+    *out = nullptr;
+    try {
+        int count = 0;
+        if(cudaGetDeviceCount(&count) != cudaSuccess || count == 0) { cudaGetLastError(); return MSA_ERR_NO_DEVICE; }
+        if(device < 0 || device >= count) return MSA_ERR_INVALID;
+        if(cudaSetDevice(device) != cudaSuccess) { cudaGetLastError(); return MSA_ERR_CUDA; }
+        cudaDeviceProp prop;
+        if(cudaGetDeviceProperties(&prop, device) != cudaSuccess) { cudaGetLastError(); return MSA_ERR_CUDA; }
+        if(prop.major < 10) return MSA_ERR_NO_DEVICE;   // built for sm_100a only
+        auto *ctx = new msa_ctx;
+        ctx->device = device;
+        ctx->num_sms = prop.multiProcessorCount;
+        ctx->cc_major = prop.major;
+        ctx->cc_minor = prop.minor;
+        if(cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            delete ctx;
+            return MSA_ERR_CUDA;
+        }
+        ctx->stream = ctx->own_stream;
+        for(auto &e : ctx->ev) cudaEventCreate(&e);
+        *out = ctx;
+        return MSA_OK;
+    } catch(const std::bad_alloc &) {
+        return MSA_ERR_NOMEM;
+    } catch(...) {
+        return MSA_ERR_CUDA;
+    }
+}
+
+void msa_destroy(msa_ctx *ctx)
+{
+    if(!ctx) return;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    release_graphs(ctx);
+    for(auto &kv : ctx->stores) free_store(kv.second);
+    ctx->prof.release();
+    ctx->bound.release();
+    ctx->tasks.release();
+    ctx->counters.release();
+    ctx->out_tmp.release();
+    ctx->pairs.release();
+    ctx->nj_buf.release();
+    for(auto &e : ctx->ev) if(e) cudaEventDestroy(e);
+    if(ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+}
+
+const char *msa_last_error(const msa_ctx *ctx) { return ctx ? ctx->err.c_str() : ""; }
+
+int msa_set_stream(msa_ctx *ctx, void *stream)
+{
+    if(!ctx) return MSA_ERR_INVALID;
+    ctx->stream = stream ? (cudaStream_t) stream : ctx->own_stream;
+    return MSA_OK;
+}
+
+void *msa_get_stream(msa_ctx *ctx) { return ctx ? (void *) ctx->stream : nullptr; }
+
+uint64_t msa_launch_count(const msa_ctx *ctx) { return ctx ? ctx->launches : 0; }
+
+int msa_seqs_upload(msa_ctx *ctx, const uint8_t *units, const uint64_t *offs, const uint64_t *lens,
+                    uint32_t n, msa_seqs *out)
+{
+    if(!ctx || !out || (n && (!offs || !lens))) return MSA_ERR_INVALID;
+    SeqStore *st = nullptr;
+    try {
+        cudaSetDevice(ctx->device);
+        st = new SeqStore;
+        st->n = n;
+        st->len.resize(n);
+        st->eff.resize(n);
+        st->plen.resize(n);
+        st->dirty.resize(n);
+        st->has_gap.resize(n);
+        st->off.resize(n);
+        uint64_t total = 0;
+        for(uint32_t i = 0; i < n; ++i) {
+            const uint64_t L = lens[i];
+            if(L >= (1ull << 30)) { free_store(st); return set_error(ctx, MSA_ERR_TOO_LARGE, "sequence longer than 2^30 units"); }
+            if(L && !units) { free_store(st); return MSA_ERR_INVALID; }
+            st->len[i] = L;
+            st->plen[i] = (uint32_t) ((L + 2) / 3 * 3);
+            st->off[i] = total;
+            total += round_up(st->plen[i] + kUnitPad, 16);
+        }
+        st->units_bytes = total + kUnitPad;
+        std::vector<uint8_t> host(st->units_bytes, (uint8_t) MSA_UNIT_END);
+        for(uint32_t i = 0; i < n; ++i) {
+            const uint8_t *src = units + offs[i];
+            uint8_t *dst = host.data() + st->off[i];
+            uint32_t first_end = st->plen[i];
+            bool seen_end = false, dirty = false, gap = false;
+            for(uint64_t k = 0; k < st->len[i]; ++k) {
+                const uint8_t u = src[k];
+                if(u > MSA_UNIT_GAP) { free_store(st); return set_error(ctx, MSA_ERR_INVALID, "unit code above 25"); }
+                dst[k] = u;
+                if(u == MSA_UNIT_END) {
+                    if(!seen_end) { first_end = (uint32_t) k; seen_end = true; }
+                } else if(seen_end) {
+                    dirty = true;
+                }
+                if(u == MSA_UNIT_GAP) gap = true;
+            }
+            if(!seen_end && st->len[i] < st->plen[i]) first_end = (uint32_t) st->len[i];
+            st->eff[i] = first_end;
+            st->has_gap[i] = gap;
+            st->dirty[i] = (dirty || first_end == 0 || gap) ? 1 : 0;
+            st->any_gap |= gap;
+        }
+        // Clean sequences sorted by effective length, longest first.
+        for(uint32_t i = 0; i < n; ++i) if(!st->dirty[i]) st->clean_sorted.push_back(i);
+        std::stable_sort(st->clean_sorted.begin(), st->clean_sorted.end(),
+                         [st](uint32_t a, uint32_t b) { return st->eff[a] > st->eff[b]; });
+        // Profile geometry.
+        st->prof_off.resize(n);
+        st->prof_lp.resize(n);
+        uint64_t poff = 0;
+        for(uint32_t i = 0; i < n; ++i) {
+            st->prof_lp[i] = (uint32_t) round_up(std::max<uint32_t>(st->eff[i], 1), kProfPad);
+            st->prof_off[i] = poff;
+            poff += (uint64_t) kAlpha * st->prof_lp[i];
+        }
+        st->prof_bytes = poff;
+
+        auto dmalloc = [&](void **p, size_t b) { return cudaMalloc(p, std::max<size_t>(b, 16)); };
+        cudaError_t e = cudaSuccess;
+        if(!e) e = dmalloc((void **) &st->d_units, st->units_bytes);
+        if(!e) e = dmalloc((void **) &st->d_off, n * sizeof(uint64_t));
+        if(!e) e = dmalloc((void **) &st->d_eff, n * sizeof(uint32_t));
+        if(!e) e = dmalloc((void **) &st->d_plen, n * sizeof(uint32_t));
+        if(!e) e = dmalloc((void **) &st->d_clean_sorted, st->clean_sorted.size() * sizeof(uint32_t));
+        if(!e) e = dmalloc((void **) &st->d_prof_off, n * sizeof(uint64_t));
+        if(!e) e = dmalloc((void **) &st->d_prof_lp, n * sizeof(uint32_t));
+        cudaStream_t s = ctx->stream;
+        if(!e) e = cudaMemcpyAsync(st->d_units, host.data(), st->units_bytes, cudaMemcpyHostToDevice, s);
+        if(!e && n) e = cudaMemcpyAsync(st->d_off, st->off.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, s);
+        if(!e && n) e = cudaMemcpyAsync(st->d_eff, st->eff.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+        if(!e && n) e = cudaMemcpyAsync(st->d_plen, st->plen.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+        if(!e && !st->clean_sorted.empty())
+            e = cudaMemcpyAsync(st->d_clean_sorted, st->clean_sorted.data(), st->clean_sorted.size() * sizeof(uint32_t),
+                                cudaMemcpyHostToDevice, s);
+        if(!e && n) e = cudaMemcpyAsync(st->d_prof_off, st->prof_off.data(), n * sizeof(uint64_t), cudaMemcpyHostToDevice, s);
+        if(!e && n) e = cudaMemcpyAsync(st->d_prof_lp, st->prof_lp.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
+        if(!e) e = cudaStreamSynchronize(s);   // host staging buffer goes out of scope
+        if(e) { free_store(st); return cuda_error(ctx, e, "sequence upload"); }
+        const uint64_t h = ctx->next_handle++;
+        ctx->stores[h] = st;
+        *out = h;
+        return MSA_OK;
+    } catch(const std::bad_alloc &) {
+        free_store(st);
+        return set_error(ctx, MSA_ERR_NOMEM, "host allocation failed");
+    } catch(...) {
+        free_store(st);
+        return set_error(ctx, MSA_ERR_CUDA, "unexpected failure in msa_seqs_upload");
+    }
+}
+
+int msa_seqs_release(msa_ctx *ctx, msa_seqs seqs)
+{
+    if(!ctx) return MSA_ERR_INVALID;
+    auto it = ctx->stores.find(seqs);
+    if(it == ctx->stores.end()) return MSA_ERR_HANDLE;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    free_store(it->second);
+    ctx->stores.erase(it);
+    return MSA_OK;
+}
+
+int64_t msa_seqs_count(msa_ctx *ctx, msa_seqs seqs)
+{
+    if(!ctx) return -1;
+    auto it = ctx->stores.find(seqs);
+    return it == ctx->stores.end() ? -1 : (int64_t) it->second->n;
+}
+
+int msa_nw_all_pairs(msa_ctx *ctx, msa_seqs seqs, const msa_table *table, int mode, int32_t *out,
+                     int out_on_device)
+{
+    if(!ctx || !table) return MSA_ERR_INVALID;
+    try {
+        auto it = ctx->stores.find(seqs);
+        if(it == ctx->stores.end()) return set_error(ctx, MSA_ERR_HANDLE, "unknown sequence store");
+        SeqStore *st = it->second;
+        if(mode != MSA_NW_AUTO && mode != MSA_NW_PLAIN && mode != MSA_NW_PERSISTENT)
+            return set_error(ctx, MSA_ERR_UNKNOWN_ALGORITHM, "unknown NW mode");
+        if(mode == MSA_NW_AUTO) mode = MSA_NW_PERSISTENT;
+        cudaSetDevice(ctx->device);
+        ExtTable ext;
+        std::string err;
+        int rc = make_ext_table(table, &ext, &err);
+        if(rc) return set_error(ctx, rc, err);
+        // A GAP unit is scored through the reference's flat table storage; where
+        // that read leaves the storage the reference is undefined.
+        if(st->any_gap) {
+            for(int x = 0; x < kAlpha; ++x)
+                for(int y = 0; y < kAlpha; ++y)
+                    if((x == MSA_UNIT_GAP || y == MSA_UNIT_GAP) && x != MSA_UNIT_END && y != MSA_UNIT_END &&
+                       !ext.valid[x * kAlpha + y])
+                        return set_error(ctx, MSA_ERR_UNDEFINED,
+                                         "GAP unit with this table reads past the reference's table storage");
+        }
+        // Exact parity with float scores needs |score| < 2^24; int32 needs < 2^31.
+        uint64_t maxlen = 0;
+        for(uint32_t i = 0; i < st->n; ++i) maxlen = std::max<uint64_t>(maxlen, st->plen[i]);
+        const int64_t vb = (int64_t) (2 * maxlen + 2048 + 2) * std::max<int64_t>(ext.max_abs, ext.penalty);
+        if(vb >= (1ll << 30)) return set_error(ctx, MSA_ERR_TOO_LARGE, "scores could exceed the int32 range");
+        // Tables that are not symmetric make the score depend on orientation:
+        // route every pair through the reference-orientation path.
+        bool symmetric = true;
+        for(int x = 0; x < 25 && symmetric; ++x)
+            for(int y = 0; y < 25; ++y)
+                if(ext.score[x * kAlpha + y] != ext.score[y * kAlpha + x]) { symmetric = false; break; }
+        std::vector<uint8_t> saved_dirty;
+        std::vector<uint32_t> saved_sorted;
+        if(!symmetric) {
+            saved_dirty = st->dirty;
+            saved_sorted = st->clean_sorted;
+            std::fill(st->dirty.begin(), st->dirty.end(), 1);
+            st->clean_sorted.clear();
+        }
+        const uint64_t npairs = (uint64_t) st->n * (st->n ? st->n - 1 : 0) / 2;
+        int32_t *d_out = out;
+        if(!out_on_device && npairs) {
+            cudaError_t e = ctx->out_tmp.ensure(npairs * sizeof(int32_t));
+            if(e) return cuda_error(ctx, e, "output buffer");
+            d_out = (int32_t *) ctx->out_tmp.ptr;
+        }
+        if(npairs && !out) return MSA_ERR_INVALID;
+        rc = nw_run(ctx, st, ext, mode, d_out);
+        if(!symmetric) {
+            st->dirty = saved_dirty;
+            st->clean_sorted = saved_sorted;
+        }
+        if(rc) return rc;
+        if(!out_on_device && npairs) {
+            cudaError_t e = cudaMemcpyAsync(out, d_out, npairs * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
+            if(!e) e = cudaStreamSynchronize(ctx->stream);
+            if(e) return cuda_error(ctx, e, "copy scores to host");
+        }
+        return MSA_OK;
+    } catch(const std::bad_alloc &) {
+        return set_error(ctx, MSA_ERR_NOMEM, "host allocation failed");
+    } catch(...) {
+        return set_error(ctx, MSA_ERR_CUDA, "unexpected failure in msa_nw_all_pairs");
+    }
+}
+
+int msa_nw_last_stats(const msa_ctx *ctx, msa_nw_stats *out)
+{
+    if(!ctx || !out) return MSA_ERR_INVALID;
+    *out = ctx->last;
+    return MSA_OK;
+}
+
+int msa_nj(msa_ctx *ctx, const void *tri, int tri_kind, uint32_t n, msa_otu *out_nodes)
+{
+    if(!ctx) return MSA_ERR_INVALID;
+    if(n < 2) return MSA_OK;
+    if(!tri || !out_nodes) return MSA_ERR_INVALID;
+    if(tri_kind < MSA_TRI_F32_HOST || tri_kind > MSA_TRI_I32_DEVICE) return MSA_ERR_INVALID;
+    try {
+        cudaSetDevice(ctx->device);
+        return nj_run(ctx, tri, tri_kind, n, out_nodes);
+    } catch(const std::bad_alloc &) {
+        return set_error(ctx, MSA_ERR_NOMEM, "host allocation failed");
+    } catch(...) {
+        return set_error(ctx, MSA_ERR_CUDA, "unexpected failure in msa_nj");
+    }
+}
+
+}  // extern "C"
+
+namespace msa {
+void release_graphs(msa_ctx *) {}
+}

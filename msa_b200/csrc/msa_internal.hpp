@@ -1,0 +1,116 @@
+// Internal declarations shared by the host runtime and the CUDA kernels of
+// libmsa_b200.so. Nothing here crosses the C ABI.
+#pragma once
+
+#include <cstdint>
+#include <cstddef>
+#include <string>
+#include <vector>
+#include <map>
+#include <mutex>
+
+#include <cuda_runtime.h>
+
+#include "../../include/msa_b200.h"
+
+namespace msa {
+
+// Profile rows: encoder units 0..25 (24 = END never scored, 25 = GAP).
+constexpr int kAlpha = 26;
+// Profile rows are padded to a multiple of the tallest strip (32 lanes x 32 rows).
+constexpr int kProfPad = 1024;
+// Every sequence's units are padded with END so 16-byte loads past the end stay in bounds.
+constexpr int kUnitPad = 64;
+
+inline uint64_t round_up(uint64_t x, uint64_t m) { return (x + m - 1) / m * m; }
+
+// Built-in tables in storage order (tables.inc).
+struct BuiltinTable {
+    const char *name;
+    int32_t penalty;
+    int8_t score[25 * 25];
+};
+const BuiltinTable *builtin_tables(int *count);
+
+// Extended 26x26 table: entry [x][y] is what the reference reads for units x, y
+// when it indexes `(*m_contents)[x][y]` on its contiguous table storage.
+// valid[x*26+y] = 0 where that read would fall outside the storage.
+struct ExtTable {
+    int8_t score[kAlpha * kAlpha];
+    uint8_t valid[kAlpha * kAlpha];
+    int32_t penalty;
+    int32_t max_abs;   // max |score| over valid entries
+};
+int make_ext_table(const msa_table *t, ExtTable *out, std::string *err);
+
+// Device-resident sequence store.
+struct SeqStore {
+    uint32_t n = 0;
+    std::vector<uint64_t> len;      // given length (units)
+    std::vector<uint32_t> eff;      // index of first END unit within the padded length
+    std::vector<uint32_t> plen;     // 3 * ceil(len / 3)
+    std::vector<uint8_t> dirty;     // END units not forming a suffix, or eff == 0
+    std::vector<uint8_t> has_gap;   // a GAP unit within the padded length
+    std::vector<uint64_t> off;      // byte offset of the units in d_units
+    uint8_t *d_units = nullptr;
+    uint64_t units_bytes = 0;
+    uint64_t *d_off = nullptr;
+    uint32_t *d_eff = nullptr;
+    uint32_t *d_plen = nullptr;
+    bool any_gap = false;
+    // Clean sequences sorted by eff descending (ties: original index ascending).
+    std::vector<uint32_t> clean_sorted;
+    uint32_t *d_clean_sorted = nullptr;
+    // Profile geometry per sequence (original index): Lp = round_up(max(eff,1), kProfPad).
+    std::vector<uint64_t> prof_off;
+    std::vector<uint32_t> prof_lp;
+    uint64_t prof_bytes = 0;
+    uint64_t *d_prof_off = nullptr;
+    uint32_t *d_prof_lp = nullptr;
+};
+
+// Growable device scratch buffer owned by a context.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t ensure(size_t need);
+    void release();
+};
+
+struct GraphCache;
+
+}  // namespace msa
+
+struct msa_ctx {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    uint64_t launches = 0;
+    std::map<uint64_t, msa::SeqStore *> stores;
+    uint64_t next_handle = 1;
+    int num_sms = 0;
+    int cc_major = 0, cc_minor = 0;
+    msa::DevBuf prof, bound, tasks, counters, out_tmp, pairs, nj_buf;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    msa_nw_stats last{};
+    msa::GraphCache *graphs = nullptr;
+};
+
+namespace msa {
+
+// Kernel launchers (nw_kernels.cu). All launch on ctx->stream and count launches.
+struct NwPlan;
+int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d_out);
+int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out);
+
+int set_error(msa_ctx *ctx, int status, const std::string &msg);
+int cuda_error(msa_ctx *ctx, cudaError_t e, const char *what);
+
+}  // namespace msa
+
+#define MSA_CUDA_TRY(ctx, call)                                             \
+    do {                                                                    \
+        cudaError_t _e = (call);                                            \
+        if(_e != cudaSuccess) return msa::cuda_error((ctx), _e, #call);     \
+    } while(0)

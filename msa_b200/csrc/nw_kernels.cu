@@ -1,0 +1,655 @@
+// All-pairs Needleman-Wunsch kernels for sm_100a.
+//
+// Recurrence (linear gap, global alignment), exactly the one of
+// sequential::align_pair (src/pairwise/needleman/impl/sequential.cpp:29-68):
+//   H[0][j] = -j*g, H[i][0] = -i*g,
+//   H[i][j] = max(H[i-1][j-1] + T[a_i][b_j], H[i][j-1] - g, H[i-1][j] - g).
+// Scores are small integers, so int32 (or, where a host-side bound proves it
+// cannot overflow, 16-bit lanes) reproduces the reference's float scores
+// exactly.
+//
+// Work layout: one warp runs one task. A task is one (rows, cols) pair, or on
+// the 16-bit path two pairs sharing the rows sequence, one per 16-bit half.
+// Lane k owns R consecutive rows of a 32*R-row strip and sweeps the columns one
+// step behind lane k-1: the cell above its first row arrives from lane k-1 by
+// __shfl_up_sync, so a strip advances one anti-diagonal per step with no
+// block-wide barrier. Strips of a long rows sequence are chained through a
+// per-warp boundary row in global memory. Substitution scores come from a
+// per-sequence score profile (one int8 row per residue code) staged per strip
+// in shared memory, laid out [code][lane][R] so that the 16-byte profile loads
+// of a warp are bank-conflict free whatever codes the lanes hold.
+#include <cstdio>
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+
+#include "msa_internal.hpp"
+
+namespace msa {
+namespace dev {
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kEnd = MSA_UNIT_END;
+
+// Sign-extended byte K of w.
+template <int K>
+__device__ __forceinline__ int32_t sbyte(uint32_t w)
+{
+    int32_t r;
+    asm("prmt.b32 %0, %1, 0, %2;" : "=r"(r) : "r"(w), "n"((K) | ((K | 8) << 4) | ((K | 8) << 8) | ((K | 8) << 12)));
+    return r;
+}
+
+// Two sign-extended bytes K of lo and hi packed as int16x2 (lo in bits 0-15).
+template <int K>
+__device__ __forceinline__ uint32_t sbyte2(uint32_t lo, uint32_t hi)
+{
+    uint32_t r;
+    asm("prmt.b32 %0, %1, %2, %3;" : "=r"(r) : "r"(lo), "r"(hi),
+        "n"((K) | ((K | 8) << 4) | ((4 + K) << 8) | (((4 + K) | 8) << 12)));
+    return r;
+}
+
+__device__ __forceinline__ uint32_t dup16(int32_t v) { return ((uint32_t) v & 0xffffu) | ((uint32_t) v << 16); }
+__device__ __forceinline__ int32_t lo16(uint32_t v) { return (int32_t) (int16_t) (v & 0xffffu); }
+__device__ __forceinline__ int32_t hi16(uint32_t v) { return (int32_t) (int16_t) (v >> 16); }
+
+// One cell: max(up - g, max(left - g, diag + s)). The inner max depends only on
+// the previous column, so the serial chain down a lane's rows is one DPX op.
+struct Wide {
+    using W = int32_t;
+    __device__ static __forceinline__ W cell(W d, W s, W left, W up, W ng)
+    {
+        const W ds = d + s;
+        const W t = __viaddmax_s32(left, ng, ds);
+        return __viaddmax_s32(up, ng, t);
+    }
+    __device__ static __forceinline__ W splat(int32_t v) { return v; }
+};
+
+struct Narrow {
+    using W = uint32_t;
+    __device__ static __forceinline__ W cell(W d, W s, W left, W up, W ng)
+    {
+        const W ds = __vadd2(d, s);
+        const W t = __viaddmax_s16x2(left, ng, ds);
+        return __viaddmax_s16x2(up, ng, t);
+    }
+    __device__ static __forceinline__ W splat(int32_t v) { return dup16(v); }
+};
+
+// R profile bytes of one lane for residue code b, from the staged strip.
+// Layout [code][plane][lane][16] with R/16 planes (R >= 16) or [code][lane][R].
+template <int R>
+struct ProfWords {
+    static constexpr int NW = R / 4;
+    uint32_t w[NW];
+    __device__ __forceinline__ void load(const int8_t *sprof, int b, int lane)
+    {
+        constexpr int SH = 32 * R;
+        if constexpr(R >= 16) {
+#pragma unroll
+            for(int p = 0; p < R / 16; ++p) {
+                const uint4 v = *reinterpret_cast<const uint4 *>(sprof + b * SH + p * 512 + lane * 16);
+                w[4 * p + 0] = v.x; w[4 * p + 1] = v.y; w[4 * p + 2] = v.z; w[4 * p + 3] = v.w;
+            }
+        } else if constexpr(R == 8) {
+            const uint2 v = *reinterpret_cast<const uint2 *>(sprof + b * SH + lane * 8);
+            w[0] = v.x; w[1] = v.y;
+        } else {
+            static_assert(R == 4, "R must be 4, 8, 16 or 32");
+            w[0] = *reinterpret_cast<const uint32_t *>(sprof + b * SH + lane * 4);
+        }
+    }
+};
+
+// Copies strip rows [i0, i0 + 32R) of a sequence profile ([code][Lp] int8,
+// global) into the warp's shared staging area.
+template <int R>
+__device__ __forceinline__ void stage_profile(int8_t *sprof, const int8_t *__restrict__ gprof,
+                                              uint32_t lp, int i0, int lane)
+{
+    constexpr int SH = 32 * R;
+    constexpr int CH = SH / 16;   // 16-byte chunks per code row
+    for(int c = lane; c < kAlpha * CH; c += 32) {
+        const int b = c / CH, w = c - b * CH;
+        const uint4 v = __ldg(reinterpret_cast<const uint4 *>(gprof + (size_t) b * lp + i0) + w);
+        int dst;
+        if constexpr(R >= 16) {
+            const int ln = w / (R / 16), pl = w - ln * (R / 16);
+            dst = b * SH + pl * 512 + ln * 16;
+        } else {
+            dst = b * SH + w * 16;   // [code][lane][R] is the natural order for R <= 16
+        }
+        *reinterpret_cast<uint4 *>(sprof + dst) = v;
+    }
+}
+
+// Runs one task on the calling warp. Column sweep: ncolsA columns of colsA in
+// the low half (or the whole word), ncolsB <= ncolsA columns of colsB in the
+// high half (Narrow only). kSkip: END units in the columns copy the left
+// neighbour (sequential.cpp:53-60) instead of scoring.
+// Returns H[nrows][ncolsA] (resA) and H[nrows][ncolsB] (resB).
+template <int R, class K, bool kSkip>
+__device__ __forceinline__ void run_task(const int8_t *__restrict__ gprof, uint32_t lp, int nrows,
+                                         const uint8_t *__restrict__ colsA, int ncolsA,
+                                         const uint8_t *__restrict__ colsB, int ncolsB,
+                                         int8_t *sprof, uint32_t *__restrict__ bound,
+                                         int32_t g, int lane, int32_t &resA, int32_t &resB)
+{
+    using W = typename K::W;
+    constexpr int SH = 32 * R;
+    constexpr bool kNarrow = std::is_same<K, Narrow>::value;
+    const int nstrips = (nrows + SH - 1) / SH;
+    const W ng = K::splat(-g);
+    int32_t outA = 0, outB = 0;
+
+    for(int s = 0; s < nstrips; ++s) {
+        const int i0 = s * SH;
+        const bool first = (s == 0);
+        const bool last = (s == nstrips - 1);
+        const int rl = nrows - 1 - i0;              // last row's offset (meaningful in the last strip)
+        const int klast = last ? rl / R : 31;
+        const int rlast = rl - (rl / R) * R;
+
+        __syncwarp();
+        stage_profile<R>(sprof, gprof, lp, i0, lane);
+        __syncwarp();
+
+        W H[R];
+#pragma unroll
+        for(int r = 0; r < R; ++r) H[r] = K::splat(-(i0 + lane * R + r + 1) * g);
+        W diag = K::splat(-(i0 + lane * R) * g);    // H[row_top - 1][0]
+        W hlast = H[R - 1];
+
+        // Boundary row of the previous strip, prefetched 32 columns at a time
+        // (lane q holds column c0 + q); lane 0 picks its column by shuffle.
+        uint32_t bq_cur = 0, bq_nxt = 0;
+        if(!first) {
+            bq_cur = bound[lane];
+            bq_nxt = bound[32 + lane];
+        }
+        int clampA = ncolsA - 1;
+        uint32_t curA = colsA[min(max(-lane, 0), clampA)];
+        uint32_t curB = 0;
+        if constexpr(kNarrow) curB = colsB[min(max(-lane, 0), ncolsB - 1)];
+
+        const int tend = ncolsA + klast;
+        for(int t = 0; t < tend; ++t) {
+            W up = __shfl_up_sync(kFull, hlast, 1);
+            if(!first) {
+                if((t & 31) == 0 && t > 0) {
+                    bq_cur = bq_nxt;
+                    bq_nxt = bound[t + 32 + lane];
+                }
+                const uint32_t bv = __shfl_sync(kFull, bq_cur, t & 31);
+                if(lane == 0) up = (W) bv;
+            } else if(lane == 0) {
+                up = K::splat(-(t + 1) * g);
+            }
+            const int j = t - lane;
+            const int jn = min(max(j + 1, 0), clampA);
+            const uint32_t nxtA = colsA[jn];
+            uint32_t nxtB = 0;
+            if constexpr(kNarrow) nxtB = colsB[min(jn, ncolsB - 1)];
+
+            if(j >= 0 && j < ncolsA) {
+                const bool skip = kSkip && curA == (uint32_t) kEnd;
+                if(!skip) {
+                    ProfWords<R> pa;
+                    pa.load(sprof, (int) curA, lane);
+                    if constexpr(kNarrow) {
+                        ProfWords<R> pb;
+                        pb.load(sprof, (int) curB, lane);
+                        W d = diag, u = up;
+#pragma unroll
+                        for(int q = 0; q < R / 4; ++q) {
+#pragma unroll
+                            for(int k = 0; k < 4; ++k) {
+                                const int r = 4 * q + k;
+                                W sc;
+                                if(k == 0) sc = sbyte2<0>(pa.w[q], pb.w[q]);
+                                else if(k == 1) sc = sbyte2<1>(pa.w[q], pb.w[q]);
+                                else if(k == 2) sc = sbyte2<2>(pa.w[q], pb.w[q]);
+                                else sc = sbyte2<3>(pa.w[q], pb.w[q]);
+                                const W h = K::cell(d, sc, H[r], u, ng);
+                                d = H[r];
+                                H[r] = h;
+                                u = h;
+                            }
+                        }
+                    } else {
+                        W d = diag, u = up;
+#pragma unroll
+                        for(int q = 0; q < R / 4; ++q) {
+#pragma unroll
+                            for(int k = 0; k < 4; ++k) {
+                                const int r = 4 * q + k;
+                                W sc;
+                                if(k == 0) sc = sbyte<0>(pa.w[q]);
+                                else if(k == 1) sc = sbyte<1>(pa.w[q]);
+                                else if(k == 2) sc = sbyte<2>(pa.w[q]);
+                                else sc = sbyte<3>(pa.w[q]);
+                                const W h = K::cell(d, sc, H[r], u, ng);
+                                d = H[r];
+                                H[r] = h;
+                                u = h;
+                            }
+                        }
+                    }
+                }
+                hlast = H[R - 1];
+                if(!last && lane == 31) bound[j] = (uint32_t) hlast;
+                if(last && lane == klast) {
+                    if(j == ncolsA - 1) {
+                        W v = H[0];
+#pragma unroll
+                        for(int r = 1; r < R; ++r) if(r == rlast) v = H[r];
+                        if constexpr(kNarrow) outA = lo16(v); else outA = (int32_t) v;
+                    }
+                    if constexpr(kNarrow) {
+                        if(j == ncolsB - 1) {
+                            W v = H[0];
+#pragma unroll
+                            for(int r = 1; r < R; ++r) if(r == rlast) v = H[r];
+                            outB = hi16(v);
+                        }
+                    }
+                }
+                diag = up;
+            }
+            curA = nxtA;
+            if constexpr(kNarrow) curB = nxtB;
+        }
+        if(last) {
+            resA = __shfl_sync(kFull, outA, klast);
+            resB = __shfl_sync(kFull, outB, klast);
+        }
+    }
+    __syncwarp();
+}
+
+__device__ __forceinline__ uint64_t tri_index(uint32_t i, uint32_t j)
+{
+    const uint64_t hi = i > j ? i : j, lo = i > j ? j : i;
+    return hi * (hi - 1) / 2 + lo;
+}
+
+}  // namespace dev
+
+// ---------------------------------------------------------------- params
+
+struct NwParams {
+    const uint8_t *units;
+    const uint64_t *uoff;
+    const uint32_t *eff;
+    const uint32_t *plen;
+    const int8_t *prof;
+    const uint64_t *poff;
+    const uint32_t *plp;
+    const uint32_t *sorted;     // clean sequences, eff descending
+    uint32_t nclean;
+    const uint64_t *row_task;   // persistent: first task of each sorted row (nclean + 1)
+    const uint8_t *row_narrow;  // persistent: 16-bit tasks for this row
+    uint64_t ntasks;
+    const uint32_t *gpairs;     // generic path: (rows orig, cols orig) pairs
+    uint64_t ngeneric;
+    uint32_t *bound;            // per resident warp: bound_stride words
+    uint64_t bound_stride;
+    int32_t *out;
+    int32_t g;
+    unsigned long long *counter;
+};
+
+// Sorted-space pair (a, b), a < b, from its a-major linear index k.
+__device__ __forceinline__ void decode_pair(uint64_t k, uint32_t n, uint32_t &a, uint32_t &b)
+{
+    // Row a starts at a*(2n - a - 1)/2.
+    const double nn = (double) n - 0.5;
+    double x = nn - sqrt(nn * nn - 2.0 * (double) k);
+    int64_t aa = (int64_t) floor(x);
+    if(aa < 0) aa = 0;
+    auto start = [n](int64_t r) -> uint64_t { return (uint64_t) r * (2 * (uint64_t) n - (uint64_t) r - 1) / 2; };
+    while(aa > 0 && start(aa) > k) --aa;
+    while(start(aa + 1) <= k) ++aa;
+    a = (uint32_t) aa;
+    b = (uint32_t) (aa + 1 + (k - start(aa)));
+}
+
+template <int R>
+__device__ __forceinline__ void clean_pair_task(const NwParams &p, uint32_t a, uint32_t b,
+                                                int8_t *sprof, uint32_t *bound, int lane)
+{
+    const uint32_t ri = p.sorted[a], ci = p.sorted[b];
+    int32_t ra = 0, rb = 0;
+    dev::run_task<R, dev::Wide, false>(p.prof + p.poff[ri], p.plp[ri], (int) p.eff[ri],
+                                       p.units + p.uoff[ci], (int) p.eff[ci], nullptr, 0,
+                                       sprof, bound, p.g, lane, ra, rb);
+    if(lane == 0) p.out[dev::tri_index(ri, ci)] = ra;
+}
+
+// Plain: one launch per length bucket (a range of the a-major pair order),
+// each warp takes pairs k_lo + w, k_lo + w + W, ... in a fixed stride.
+template <int R, int WPB>
+__global__ void __launch_bounds__(WPB * 32) nw_plain_kernel(NwParams p, uint64_t k_lo, uint64_t k_hi)
+{
+    extern __shared__ __align__(16) int8_t smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int8_t *sprof = smem + warp * (kAlpha * 32 * R);
+    const uint64_t gw = (uint64_t) blockIdx.x * WPB + warp;
+    const uint64_t nw = (uint64_t) gridDim.x * WPB;
+    uint32_t *bound = p.bound + gw * p.bound_stride;
+    for(uint64_t k = k_lo + gw; k < k_hi; k += nw) {
+        uint32_t a, b;
+        decode_pair(k, p.nclean, a, b);
+        clean_pair_task<R>(p, a, b, sprof, bound, lane);
+    }
+}
+
+// Persistent: one launch over every clean task in cost order (rows longest
+// first); warps take the next task from a global counter.
+template <int R, int WPB>
+__global__ void __launch_bounds__(WPB * 32) nw_persistent_kernel(NwParams p)
+{
+    extern __shared__ __align__(16) int8_t smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int8_t *sprof = smem + warp * (kAlpha * 32 * R);
+    const uint64_t gw = (uint64_t) blockIdx.x * WPB + warp;
+    uint32_t *bound = p.bound + gw * p.bound_stride;
+    for(;;) {
+        unsigned long long q = 0;
+        if(lane == 0) q = atomicAdd(p.counter, 1ull);
+        q = __shfl_sync(dev::kFull, q, 0);
+        if(q >= p.ntasks) break;
+        // Row of task q: binary search over row_task.
+        uint32_t lo = 0, hi = p.nclean - 1;
+        while(lo < hi) {
+            const uint32_t mid = (lo + hi + 1) >> 1;
+            if(p.row_task[mid] <= q) lo = mid; else hi = mid - 1;
+        }
+        const uint32_t a = lo;
+        const uint64_t t = q - p.row_task[a];
+        const uint32_t ri = p.sorted[a];
+        if(p.row_narrow[a]) {
+            const uint32_t b1 = a + 1 + (uint32_t) (2 * t);
+            const uint32_t b2 = (b1 + 1 < p.nclean) ? b1 + 1 : b1;
+            const uint32_t c1 = p.sorted[b1], c2 = p.sorted[b2];
+            int32_t r1 = 0, r2 = 0;
+            dev::run_task<R, dev::Narrow, false>(p.prof + p.poff[ri], p.plp[ri], (int) p.eff[ri],
+                                                 p.units + p.uoff[c1], (int) p.eff[c1],
+                                                 p.units + p.uoff[c2], (int) p.eff[c2],
+                                                 sprof, bound, p.g, lane, r1, r2);
+            if(lane == 0) {
+                p.out[dev::tri_index(ri, c1)] = r1;
+                if(b2 != b1) p.out[dev::tri_index(ri, c2)] = r2;
+            }
+        } else {
+            clean_pair_task<R>(p, a, a + 1 + (uint32_t) t, sprof, bound, lane);
+        }
+    }
+}
+
+// Pairs that involve a sequence with END units before its last letter, or an
+// empty one: the reference's orientation (rows = more 3-unit blocks, ties to
+// the pair's second element) and its END handling (rows stop at the first END,
+// END columns copy the left neighbour over the full padded width).
+template <int R, int WPB>
+__global__ void __launch_bounds__(WPB * 32) nw_generic_kernel(NwParams p)
+{
+    extern __shared__ __align__(16) int8_t smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    int8_t *sprof = smem + warp * (kAlpha * 32 * R);
+    const uint64_t gw = (uint64_t) blockIdx.x * WPB + warp;
+    const uint64_t nw = (uint64_t) gridDim.x * WPB;
+    uint32_t *bound = p.bound + gw * p.bound_stride;
+    for(uint64_t k = gw; k < p.ngeneric; k += nw) {
+        const uint32_t ri = p.gpairs[2 * k], ci = p.gpairs[2 * k + 1];
+        const int nrows = (int) p.eff[ri], ncols = (int) p.plen[ci];
+        int32_t ra = -ncols * p.g, rb = 0;
+        if(nrows > 0 && ncols > 0) {
+            dev::run_task<R, dev::Wide, true>(p.prof + p.poff[ri], p.plp[ri], nrows,
+                                              p.units + p.uoff[ci], ncols, nullptr, 0,
+                                              sprof, bound, p.g, lane, ra, rb);
+        } else if(nrows > 0) {
+            ra = -nrows * p.g;   // no columns: every row copies column 0
+        }
+        if(lane == 0) p.out[dev::tri_index(ri, ci)] = ra;
+    }
+}
+
+// Score profile of every sequence: prof[off + b*Lp + i] = T[unit_i][b] for
+// i < eff, 0 beyond. One block per sequence, 16 bytes per thread step.
+__global__ void build_profiles_kernel(const uint8_t *__restrict__ units, const uint64_t *__restrict__ uoff,
+                                      const uint32_t *__restrict__ eff, const uint64_t *__restrict__ poff,
+                                      const uint32_t *__restrict__ plp, const int8_t *__restrict__ ext,
+                                      int8_t *__restrict__ prof)
+{
+    __shared__ int8_t tbl[kAlpha * kAlpha];
+    for(int i = threadIdx.x; i < kAlpha * kAlpha; i += blockDim.x) tbl[i] = ext[i];
+    __syncthreads();
+    const uint32_t s = blockIdx.x;
+    const uint8_t *u = units + uoff[s];
+    const uint32_t e = eff[s], lp = plp[s];
+    int8_t *dst = prof + poff[s];
+    const uint32_t chunks = lp / 16;
+    for(uint32_t c = threadIdx.x; c < chunks * kAlpha; c += blockDim.x) {
+        const uint32_t b = c / chunks, w = c - b * chunks;
+        const uint32_t i = w * 16;
+        uint32_t out[4] = {0, 0, 0, 0};
+        if(i < e) {
+            const uint4 v = *reinterpret_cast<const uint4 *>(u + i);
+            const uint32_t in[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+            for(int q = 0; q < 4; ++q) {
+#pragma unroll
+                for(int k = 0; k < 4; ++k) {
+                    const uint32_t x = (in[q] >> (8 * k)) & 0xffu;
+                    const int8_t sc = (i + 4 * q + k < e && x < (uint32_t) kAlpha) ? tbl[x * kAlpha + b] : 0;
+                    out[q] |= ((uint32_t) (uint8_t) sc) << (8 * k);
+                }
+            }
+        }
+        *reinterpret_cast<uint4 *>(dst + (size_t) b * lp + i) = make_uint4(out[0], out[1], out[2], out[3]);
+    }
+}
+
+// ---------------------------------------------------------------- host side
+
+static constexpr int kPlainR = 16;
+static constexpr int kWPB = 4;
+
+template <int R>
+static size_t smem_bytes() { return (size_t) kWPB * kAlpha * 32 * R; }
+
+struct Launch {
+    int blocks_per_sm = 0;
+};
+
+template <class KernelT>
+static int occupancy(KernelT kernel, size_t smem, int *blocks)
+{
+    cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem);
+    if(e != cudaSuccess) return -1;
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks, kernel, kWPB * 32, smem);
+    if(e != cudaSuccess || *blocks < 1) return -1;
+    return 0;
+}
+
+// Upper bound on |H| for a task: every path of an (rows_p x cols) DP moves
+// through at most rows_p + cols cells, each changing H by at most
+// max(|score|, g); the extra 2*max covers the d+s intermediate.
+static inline int64_t value_bound(int64_t rows_p, int64_t cols, const ExtTable &t)
+{
+    const int64_t m = std::max<int64_t>(t.max_abs, t.penalty);
+    return (rows_p + cols + 2) * m;
+}
+
+int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d_out)
+{
+    cudaStream_t s = ctx->stream;
+    const uint32_t n = st->n;
+    msa_nw_stats stats{};
+    stats.pairs = (uint64_t) n * (n > 0 ? n - 1 : 0) / 2;
+    if(n < 2) { ctx->last = stats; return MSA_OK; }
+
+    MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[0], s));
+
+    // 1. Score profiles for every sequence.
+    MSA_CUDA_TRY(ctx, ctx->prof.ensure(st->prof_bytes + kAlpha * kAlpha + 64));
+    int8_t *d_prof = (int8_t *) ctx->prof.ptr;
+    int8_t *d_ext = d_prof + st->prof_bytes;
+    MSA_CUDA_TRY(ctx, cudaMemcpyAsync(d_ext, tbl.score, kAlpha * kAlpha, cudaMemcpyHostToDevice, s));
+    build_profiles_kernel<<<n, 256, 0, s>>>(st->d_units, st->d_off, st->d_eff, st->d_prof_off,
+                                            st->d_prof_lp, d_ext, d_prof);
+    MSA_CUDA_TRY(ctx, cudaGetLastError());
+    ctx->launches++;
+    stats.launches++;
+
+    // 2. Plan.
+    const uint32_t nclean = (uint32_t) st->clean_sorted.size();
+    const uint64_t nclean_pairs = (uint64_t) nclean * (nclean > 0 ? nclean - 1 : 0) / 2;
+    std::vector<uint32_t> gpairs;
+    {
+        // Pairs with at least one dirty sequence, in the reference's orientation.
+        std::vector<uint32_t> dirty;
+        for(uint32_t i = 0; i < n; ++i) if(st->dirty[i]) dirty.push_back(i);
+        if(!dirty.empty()) {
+            std::vector<uint8_t> isd(n, 0);
+            for(uint32_t d : dirty) isd[d] = 1;
+            for(uint32_t i = 1; i < n; ++i) {
+                for(uint32_t j = 0; j < i; ++j) {
+                    if(!isd[i] && !isd[j]) continue;
+                    const uint64_t bi = (st->len[i] + 2) / 3, bj = (st->len[j] + 2) / 3;
+                    const uint32_t r = bi > bj ? i : j, c = bi > bj ? j : i;
+                    gpairs.push_back(r);
+                    gpairs.push_back(c);
+                }
+            }
+        }
+    }
+    const uint64_t ngeneric = gpairs.size() / 2;
+
+    uint32_t max_cols = 1;
+    for(uint32_t i = 0; i < n; ++i) max_cols = std::max(max_cols, st->plen[i]);
+
+    NwParams p{};
+    p.units = st->d_units;
+    p.uoff = st->d_off;
+    p.eff = st->d_eff;
+    p.plen = st->d_plen;
+    p.prof = d_prof;
+    p.poff = st->d_prof_off;
+    p.plp = st->d_prof_lp;
+    p.sorted = st->d_clean_sorted;
+    p.nclean = nclean;
+    p.out = d_out;
+    p.g = tbl.penalty;
+    p.bound_stride = round_up((uint64_t) max_cols + 96, 32);
+
+    auto kplain = nw_plain_kernel<kPlainR, kWPB>;
+    auto kpers = nw_persistent_kernel<kPlainR, kWPB>;
+    auto kgen = nw_generic_kernel<kPlainR, kWPB>;
+    const size_t smem = smem_bytes<kPlainR>();
+    int bps = 0;
+    if(occupancy(kplain, smem, &bps)) return set_error(ctx, MSA_ERR_CUDA, "occupancy query failed (no sm_100a image?)");
+    int bps2 = 0, bps3 = 0;
+    if(occupancy(kpers, smem, &bps2) || occupancy(kgen, smem, &bps3))
+        return set_error(ctx, MSA_ERR_CUDA, "occupancy query failed");
+    bps = std::min(bps, std::min(bps2, bps3));
+    const uint64_t resident_blocks = (uint64_t) ctx->num_sms * (uint64_t) bps;
+    const uint64_t resident_warps = resident_blocks * kWPB;
+
+    MSA_CUDA_TRY(ctx, ctx->bound.ensure(resident_warps * p.bound_stride * sizeof(uint32_t)));
+    p.bound = (uint32_t *) ctx->bound.ptr;
+
+    MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[1], s));
+
+    if(ngeneric > 0) {
+        MSA_CUDA_TRY(ctx, ctx->pairs.ensure(gpairs.size() * sizeof(uint32_t)));
+        MSA_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->pairs.ptr, gpairs.data(), gpairs.size() * sizeof(uint32_t),
+                                          cudaMemcpyHostToDevice, s));
+        p.gpairs = (const uint32_t *) ctx->pairs.ptr;
+        p.ngeneric = ngeneric;
+        const uint64_t blocks = std::min<uint64_t>(resident_blocks, (ngeneric + kWPB - 1) / kWPB);
+        kgen<<<(unsigned) blocks, kWPB * 32, smem, s>>>(p);
+        MSA_CUDA_TRY(ctx, cudaGetLastError());
+        ctx->launches++;
+        stats.launches++;
+    }
+
+    if(nclean_pairs > 0) {
+        if(mode == MSA_NW_PLAIN) {
+            // Buckets: runs of sorted rows with the same strip count.
+            constexpr int SH = 32 * kPlainR;
+            uint32_t a = 0;
+            while(a + 1 < nclean) {
+                const uint32_t strips = (st->eff[st->clean_sorted[a]] + SH - 1) / SH;
+                uint32_t a2 = a + 1;
+                while(a2 + 1 < nclean && (st->eff[st->clean_sorted[a2]] + SH - 1) / SH == strips) ++a2;
+                const uint64_t k_lo = (uint64_t) a * (2 * (uint64_t) nclean - a - 1) / 2;
+                const uint64_t k_hi = (uint64_t) a2 * (2 * (uint64_t) nclean - a2 - 1) / 2;
+                const uint64_t warps = k_hi - k_lo;
+                const uint64_t blocks = std::min<uint64_t>(resident_blocks, (warps + kWPB - 1) / kWPB);
+                kplain<<<(unsigned) blocks, kWPB * 32, smem, s>>>(p, k_lo, k_hi);
+                MSA_CUDA_TRY(ctx, cudaGetLastError());
+                ctx->launches++;
+                stats.launches++;
+                a = a2;
+            }
+        } else {
+            // Tasks per sorted row; 16-bit tasks where the bound allows.
+            std::vector<uint64_t> row_task(nclean + 1, 0);
+            std::vector<uint8_t> row_narrow(nclean, 0);
+            constexpr int SH = 32 * kPlainR;
+            uint64_t q = 0;
+            uint32_t narrow_tasks = 0;
+            for(uint32_t a = 0; a < nclean; ++a) {
+                row_task[a] = q;
+                const uint64_t cnt = nclean - 1 - a;
+                if(cnt == 0) continue;
+                const int64_t rows_p = (int64_t) round_up(st->eff[st->clean_sorted[a]], SH);
+                const int64_t cols = st->eff[st->clean_sorted[a + 1]];
+                const bool narrow = value_bound(rows_p, cols, tbl) <= 32000;
+                row_narrow[a] = narrow ? 1 : 0;
+                const uint64_t tasks = narrow ? (cnt + 1) / 2 : cnt;
+                if(narrow) narrow_tasks += (uint32_t) tasks;
+                q += tasks;
+            }
+            row_task[nclean] = q;
+            stats.narrow_tasks = narrow_tasks;
+            const size_t tb = (nclean + 1) * sizeof(uint64_t) + nclean + 16;
+            MSA_CUDA_TRY(ctx, ctx->tasks.ensure(tb));
+            MSA_CUDA_TRY(ctx, ctx->counters.ensure(64));
+            uint64_t *d_rt = (uint64_t *) ctx->tasks.ptr;
+            uint8_t *d_rn = (uint8_t *) (d_rt + nclean + 1);
+            MSA_CUDA_TRY(ctx, cudaMemcpyAsync(d_rt, row_task.data(), (nclean + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+            MSA_CUDA_TRY(ctx, cudaMemcpyAsync(d_rn, row_narrow.data(), nclean, cudaMemcpyHostToDevice, s));
+            MSA_CUDA_TRY(ctx, cudaMemsetAsync(ctx->counters.ptr, 0, 64, s));
+            p.row_task = d_rt;
+            p.row_narrow = d_rn;
+            p.ntasks = q;
+            p.counter = (unsigned long long *) ctx->counters.ptr;
+            const uint64_t blocks = std::min<uint64_t>(resident_blocks, (q + kWPB - 1) / kWPB);
+            kpers<<<(unsigned) std::max<uint64_t>(blocks, 1), kWPB * 32, smem, s>>>(p);
+            MSA_CUDA_TRY(ctx, cudaGetLastError());
+            ctx->launches++;
+            stats.launches++;
+        }
+    }
+
+    MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[2], s));
+    MSA_CUDA_TRY(ctx, cudaEventSynchronize(ctx->ev[2]));
+    float ms_k = 0, ms_t = 0;
+    cudaEventElapsedTime(&ms_k, ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&ms_t, ctx->ev[0], ctx->ev[2]);
+    stats.kernel_ms = ms_k;
+    stats.total_ms = ms_t;
+    uint64_t cells = 0;
+    for(uint32_t i = 1; i < n; ++i)
+        for(uint32_t j = 0; j < i; ++j) cells += st->len[i] * st->len[j];
+    stats.cells = cells;
+    ctx->last = stats;
+    return MSA_OK;
+}
+
+}  // namespace msa

@@ -1,0 +1,147 @@
+"""All-pairs NW on the GPU through the C ABI, checked bit-exact against the
+reference (golden fixtures it produced) and the oracle restatement."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from msa_b200 import Database, ScoringTable, pairwise
+from msa_b200 import _lib
+from msa_b200 import workloads as W
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+MODES = [_lib.MSA_NW_PLAIN, _lib.MSA_NW_PERSISTENT]
+
+
+def gpu_scores(wl, table, mode, pad3=False):
+    flat, offs, lens = wl.flat_units(pad3=pad3)
+    t = table if isinstance(table, ScoringTable) else ScoringTable(table)
+    return pairwise.score_units(flat, offs, lens, t, mode)
+
+
+@pytest.fixture(scope="module")
+def tables(golden):
+    return O.table_block(golden)
+
+
+def oracle_scores(wl, table, tables, pad3=False):
+    flat, offs, lens = wl.flat_units(pad3=pad3)
+    return O.oracle_nw_all_pairs(flat, offs, lens, tables, 7, O.TABLE_INDEX[table], O.PENALTY[table])
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_c1_matches_reference(gpu, golden, mode):
+    got = gpu_scores(W.c1(), "blosum62", mode)
+    assert np.array_equal(got, np.array(golden["c1"]["scores"], np.int32))
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_edge_sets_match_reference(gpu, golden, mode):
+    for e in golden["edge"]:
+        wl = W.random_set(e["seed"], e["n"], e["lo"], e["hi"], alphabet=e["alphabet"].encode(),
+                          extra=e["extra"].encode("latin-1"))
+        for pad3 in (False, True):
+            got = gpu_scores(wl, e["table"], mode, pad3)
+            assert np.array_equal(got, np.array(e["scores"], np.int32)), (e["seed"], pad3)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("seed,n,lo,hi,table", [
+    (41, 40, 1, 70, "blosum62"),        # single strips, tiny columns
+    (42, 12, 480, 1100, "default"),     # strip boundaries at 512 / 1024 rows
+    (43, 9, 1500, 2600, "pam250"),      # several strips, wide columns
+    (44, 33, 500, 530, "blosum45"),     # odd count: unpaired 16-bit task
+    (45, 6, 5000, 7000, "blosum62"),    # 32-bit path (16-bit bound exceeded)
+])
+def test_random_sets_match_oracle(gpu, tables, mode, seed, n, lo, hi, table):
+    alpha = b"ACGTN" if table == "default" else b"ARNDCQEGHILKMFPSTWYV"
+    wl = W.random_set(seed, n, lo, hi, alphabet=alpha)
+    got = gpu_scores(wl, table, mode)
+    assert np.array_equal(got, oracle_scores(wl, table, tables))
+
+
+def test_plain_and_persistent_agree_on_related_sequences(gpu):
+    wl = W.c2(n=300)
+    a = gpu_scores(wl, "blosum62", _lib.MSA_NW_PLAIN)
+    b = gpu_scores(wl, "blosum62", _lib.MSA_NW_PERSISTENT)
+    assert np.array_equal(a, b)
+
+
+@pytest.mark.parametrize("name", ["c2", "c4"])
+def test_full_workload_samples_match_reference(gpu, golden, name):
+    g = golden[name + "_sample"]
+    wl = W.BY_NAME[name]()
+    got = gpu_scores(wl, g["table"], _lib.MSA_NW_PERSISTENT)
+    i, j = np.array(g["i"], np.int64), np.array(g["j"], np.int64)
+    assert np.array_equal(got[i * (i - 1) // 2 + j], np.array(g["scores"], np.int32))
+
+
+def test_c3_full_plain_equals_persistent_and_reference_sample(gpu, golden):
+    g = golden["c3_sample"]
+    wl = W.c3()
+    pers = gpu_scores(wl, "default", _lib.MSA_NW_PERSISTENT)
+    i, j = np.array(g["i"], np.int64), np.array(g["j"], np.int64)
+    assert np.array_equal(pers[i * (i - 1) // 2 + j], np.array(g["scores"], np.int32))
+    plain = gpu_scores(wl, "default", _lib.MSA_NW_PLAIN)
+    assert np.array_equal(plain, pers)
+
+
+def test_asymmetric_custom_table_uses_reference_orientation(gpu):
+    rng = np.random.default_rng(7)
+    m = rng.integers(-6, 7, (25, 25)).astype(np.int32)
+    t = ScoringTable.custom(m, 3)
+    wl = W.random_set(46, 20, 1, 90)
+    got = gpu_scores(wl, t, _lib.MSA_NW_PERSISTENT)
+    flat, offs, lens = wl.flat_units()
+    want = O.oracle_nw_all_pairs(flat, offs, lens, m.reshape(-1), 1, 0, 3)
+    assert np.array_equal(got, want)
+
+
+def test_output_on_device(gpu, golden):
+    import torch
+    wl = W.c1()
+    flat, offs, lens = wl.flat_units()
+    lib = _lib.lib()
+    h = ctypes.c_uint64()
+    u8, u64 = ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint64)
+    _lib.check(lib.msa_seqs_upload(gpu.handle, flat.ctypes.data_as(u8), offs.ctypes.data_as(u64),
+                                   lens.ctypes.data_as(u64), wl.n, ctypes.byref(h)), gpu.handle)
+    out = torch.zeros(wl.n * (wl.n - 1) // 2, dtype=torch.int32, device="cuda:0")
+    t = ScoringTable("blosum62")
+    _lib.check(lib.msa_nw_all_pairs(gpu.handle, h.value, ctypes.byref(t._t), _lib.MSA_NW_PERSISTENT,
+                                    ctypes.c_void_p(out.data_ptr()), 1), gpu.handle)
+    torch.cuda.synchronize()
+    lib.msa_seqs_release(gpu.handle, h.value)
+    assert np.array_equal(out.cpu().numpy(), np.array(golden["c1"]["scores"], np.int32))
+
+
+def test_gap_unit_with_pam250_is_rejected(gpu):
+    wl = W.random_set(47, 5, 5, 10, extra=b"-")
+    flat, offs, lens = wl.flat_units()
+    with pytest.raises(_lib.MsaError) as ei:
+        pairwise.score_units(flat, offs, lens, ScoringTable("pam250"))
+    assert ei.value.status == _lib.MSA_ERR_UNDEFINED
+
+
+def test_database_run_api(gpu, golden):
+    db = Database()
+    for k, s in enumerate(W.c1().seqs):
+        db.add((f"s{k}", bytes(s)))
+    dm = pairwise.run(db, table="blosum62", algorithm="default")
+    want = golden["c1"]["scores"]
+    assert dm.count == 16
+    assert all(dm[i, j] == want[i * (i - 1) // 2 + j] for i in range(1, 16) for j in range(i))
+    dm2 = pairwise.run(db, table="blosum62", algorithm="sequential")
+    assert np.array_equal(dm.scores, dm2.scores)
+
+
+def test_stats_and_launch_counts(gpu):
+    wl = W.c2(n=200)
+    before = gpu.launches
+    gpu_scores(wl, "blosum62", _lib.MSA_NW_PERSISTENT)
+    s = pairwise.last_stats()
+    assert s.pairs == 200 * 199 // 2 and s.cells == wl.cells()
+    assert s.launches >= 2 and gpu.launches - before == s.launches
+    assert s.narrow_tasks > 0 and s.kernel_ms > 0
