@@ -164,6 +164,43 @@ def reference_arm(args):
 
 # ---------------------------------------------------------------- GPU arm
 
+PROBE_OPS = ["iadd", "imnmx", "viaddmax_s32", "vimax3_s32", "vadd2", "viaddmax_s16x2", "vimax3_s16x2",
+             "viaddmax_u16x2", "vimax3_u16x2", "vmaxu2", "prmt", "cell_s32", "cell_s16x2", "cell_u16x2_biased"]
+
+
+def probe_ops(iters: int = 2048) -> dict:
+    """Lane-ops per SM per clock of each integer form (msa_probe_op)."""
+    import ctypes
+
+    from msa_b200 import _lib, runtime
+    ctx = runtime.context(0)
+    res = {}
+    for k, name in enumerate(PROBE_OPS):
+        p = _lib.MsaOpProbe()
+        _lib.check(_lib.lib().msa_probe_op(ctx.handle, k, iters, ctypes.byref(p)), ctx.handle)
+        res[name] = {"ops_per_clk_sm": round(p.ops_per_clk_sm, 2), "sm_mhz": round(p.sm_clock_mhz, 1)}
+    print(json.dumps(res))
+    return res
+
+
+def profile_run(args):
+    """One scoring call (after warm-up) for ncu captures; prints its stats."""
+    import ctypes
+
+    from msa_b200 import ScoringTable, _lib, pairwise
+    wl = load_workload(args.workload)
+    if args.n:
+        wl.seqs = wl.seqs[:args.n]
+    flat, offs, lens = wl.flat_units()
+    mode = _lib.MSA_NW_PERSISTENT if args.profile == "persistent" else _lib.MSA_NW_PLAIN
+    for _ in range(args.warmup + 1):
+        pairwise.score_units(flat, offs, lens, ScoringTable(wl.table), mode)
+    st = pairwise.last_stats()
+    print(json.dumps({"workload": args.workload, "n": wl.n, "mode": args.profile, "cells": wl.cells(),
+                      "kernel_ms": st.kernel_ms, "gcups": wl.cells() / st.kernel_ms / 1e6,
+                      "launches": st.launches, "narrow_tasks": st.narrow_tasks}))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -174,9 +211,17 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--cpu-cells", type=float, default=1.5e10)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile", choices=["persistent", "plain"], default=None,
+                    help="profiling run: --warmup calls then one call, on the first --n sequences")
+    ap.add_argument("--n", type=int, default=0, help="with --profile: use the first N sequences")
+    ap.add_argument("--probe", action="store_true", help="integer-op throughput probes (lane-ops/clk/SM)")
     args = ap.parse_args()
+    if args.probe:
+        return probe_ops()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.profile:
+        return profile_run(args)
 
     import ctypes
 

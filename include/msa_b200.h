@@ -147,6 +147,11 @@ typedef enum msa_nw_mode {
 int msa_nw_all_pairs(msa_ctx *ctx, msa_seqs seqs, const msa_table *table, int mode,
                      int32_t *out, int out_on_device);
 
+/* Tile shape of the persistent kernel: rows per lane (16 or 32) and warps per
+ * CTA (4 or 8); 0, 0 restores the committed autotuned choice. No counterpart
+ * in the reference (its one kernel shape is fixed, hybrid.cu:57). */
+int msa_nw_set_tiles(msa_ctx *ctx, int rows_per_lane, int warps_per_cta);
+
 /* Timing breakdown of the context's last msa_nw_all_pairs call (device ms). */
 typedef struct msa_nw_stats {
     double kernel_ms;       /* NW kernels only */
@@ -188,6 +193,23 @@ typedef enum msa_tri_kind {
  * n < 2 writes nothing (phylogeny returns an empty tree).
  */
 int msa_nj(msa_ctx *ctx, const void *tri, int tri_kind, uint32_t n, msa_otu *out_nodes);
+
+/* ------------------------------------------------------------ diagnostics */
+
+/*
+ * Throughput of one integer operation form (no counterpart in the reference;
+ * it measures the INT32 issue roofline the NW kernels are reported against).
+ * op: 0 IADD, 1 IMNMX, 2 viaddmax_s32, 3 vimax3_s32, 4 vadd2, 5 viaddmax_s16x2,
+ * 6 vimax3_s16x2, 7 viaddmax_u16x2, 8 vimax3_u16x2, 9 vmaxu2, 10 PRMT,
+ * 11 the 32-bit NW cell, 12 the signed 16x2 NW cell, 13 the biased 16x2 cell.
+ */
+typedef struct msa_op_probe {
+    double ops_per_clk_sm;  /* lane-operations per SM per SM clock */
+    double ms;              /* kernel time of the measured launch */
+    uint64_t lane_ops;
+    double sm_clock_mhz;    /* SM cycles / elapsed time during the launch */
+} msa_op_probe;
+int msa_probe_op(msa_ctx *ctx, int op, int iters, msa_op_probe *out);
 
 #ifdef __cplusplus
 }

@@ -69,6 +69,11 @@ class MsaJobStats(ctypes.Structure):
                 ("cells", ctypes.c_uint64), ("n", ctypes.c_uint32), ("launches", ctypes.c_uint32)]
 
 
+class MsaOpProbe(ctypes.Structure):
+    _fields_ = [("ops_per_clk_sm", ctypes.c_double), ("ms", ctypes.c_double), ("lane_ops", ctypes.c_uint64),
+                ("sm_clock_mhz", ctypes.c_double)]
+
+
 class MsaError(RuntimeError):
     """A non-zero msa_status from the library."""
 
@@ -100,9 +105,11 @@ _PROTOS = [
     ("msa_seqs_count", ctypes.c_int64, [ctypes.c_void_p, ctypes.c_uint64]),
     ("msa_nw_all_pairs", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(MsaTable), ctypes.c_int,
                                         ctypes.c_void_p, ctypes.c_int]),
+    ("msa_nw_set_tiles", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     ("msa_nw_last_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(MsaNwStats)]),
     ("msa_nj", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32,
                               ctypes.POINTER(MsaOtu)]),
+    ("msa_probe_op", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(MsaOpProbe)]),
     ("msa_serve_start", ctypes.c_int, [ctypes.POINTER(MsaServeConfig), ctypes.POINTER(ctypes.c_void_p)]),
     ("msa_serve_submit", ctypes.c_int, [ctypes.c_void_p, c_u8p, c_u64p, c_u64p, ctypes.c_uint32,
                                         ctypes.POINTER(MsaTable), ctypes.POINTER(ctypes.c_uint64)]),

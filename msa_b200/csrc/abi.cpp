@@ -143,7 +143,7 @@ int msa_seqs_upload(msa_ctx *ctx, const uint8_t *units, const uint64_t *offs, co
         st->dirty.resize(n);
         st->has_gap.resize(n);
         st->off.resize(n);
-        uint64_t total = 0;
+        uint64_t total = kUnitFront;   // lanes may read a few residues before a sequence
         for(uint32_t i = 0; i < n; ++i) {
             const uint64_t L = lens[i];
             if(L >= (1ull << 30)) { free_store(st); return set_error(ctx, MSA_ERR_TOO_LARGE, "sequence longer than 2^30 units"); }
@@ -315,6 +315,17 @@ int msa_nw_all_pairs(msa_ctx *ctx, msa_seqs seqs, const msa_table *table, int mo
     } catch(...) {
         return set_error(ctx, MSA_ERR_CUDA, "unexpected failure in msa_nw_all_pairs");
     }
+}
+
+int msa_nw_set_tiles(msa_ctx *ctx, int rows_per_lane, int warps_per_cta)
+{
+    if(!ctx) return MSA_ERR_INVALID;
+    if(rows_per_lane == 0 && warps_per_cta == 0) { ctx->tile_r = ctx->tile_w = 0; return MSA_OK; }
+    if((rows_per_lane != 16 && rows_per_lane != 32) || (warps_per_cta != 4 && warps_per_cta != 8))
+        return MSA_ERR_INVALID;
+    ctx->tile_r = rows_per_lane;
+    ctx->tile_w = warps_per_cta;
+    return MSA_OK;
 }
 
 int msa_nw_last_stats(const msa_ctx *ctx, msa_nw_stats *out)

@@ -39,7 +39,9 @@ struct ExtTable {
     int8_t score[kAlpha * kAlpha];
     uint8_t valid[kAlpha * kAlpha];
     int32_t penalty;
-    int32_t max_abs;   // max |score| over valid entries
+    int32_t max_abs;   // max |score| over valid entries (END row/column excluded)
+    int32_t max_pos;   // largest score
+    int32_t max_neg;   // largest magnitude of a negative score
 };
 int make_ext_table(const msa_table *t, ExtTable *out, std::string *err);
 
@@ -95,6 +97,7 @@ struct msa_ctx {
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     msa_nw_stats last{};
     msa::GraphCache *graphs = nullptr;
+    int tile_r = 0, tile_w = 0;   // persistent-kernel tile override (0 = autotuned)
 };
 
 namespace msa {
@@ -102,6 +105,8 @@ namespace msa {
 // Kernel launchers (nw_kernels.cu). All launch on ctx->stream and count launches.
 struct NwPlan;
 int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d_out);
+// Bytes of padding before the first sequence in a store's unit buffer.
+constexpr int kUnitFront = 64;
 int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out);
 
 int set_error(msa_ctx *ctx, int status, const std::string &msg);

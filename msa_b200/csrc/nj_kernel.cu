@@ -203,8 +203,13 @@ __global__ void __launch_bounds__(kThreads) nj_kernel(State st)
                 const float pairsum = __fsub_rn(Sl[x], Sl[y]);
                 const float den = (float) (2u * (c - 2));
                 const float q = __fdiv_rn(pairsum, den);
-                const float dx = __double2float_rn(__dadd_rn(__dmul_rn(0.5, (double) dxy), (double) q));
-                const float dy = __fsub_rn(dxy, dx);
+                float dx = __double2float_rn(__dadd_rn(__dmul_rn(0.5, (double) dxy), (double) q));
+                float dy = __fsub_rn(dxy, dx);
+                // The last join divides by 2(c-2) = 0; for 0/0 the reference's x86
+                // SSE arithmetic yields the default NaN 0xFFC00000 and propagates it
+                // into dx and dy, where the GPU would give its canonical 0x7FFFFFFF.
+                if(dx != dx) dx = __uint_as_float(0xFFC00000u);
+                if(dy != dy) dy = __uint_as_float(0xFFC00000u);
                 st.rec_x[step] = __ldcg(st.map + px);
                 st.rec_y[step] = __ldcg(st.map + py);
                 st.rec_dx[step] = dx;

@@ -65,6 +65,10 @@ struct Wide {
         return __viaddmax_s32(up, ng, t);
     }
     __device__ static __forceinline__ W splat(int32_t v) { return v; }
+    // max(left - g, diag + s): the part of a cell that needs only the previous column.
+    __device__ static __forceinline__ W cell_part(W d, W s, W left, W ng) { return __viaddmax_s32(left, ng, d + s); }
+    // max(up - g, part): the serial part down a lane's rows.
+    __device__ static __forceinline__ W cell_chain(W up, W ng, W part) { return __viaddmax_s32(up, ng, part); }
 };
 
 struct Narrow {
@@ -76,6 +80,8 @@ struct Narrow {
         return __viaddmax_s16x2(up, ng, t);
     }
     __device__ static __forceinline__ W splat(int32_t v) { return dup16(v); }
+    __device__ static __forceinline__ W cell_part(W d, W s, W left, W ng) { return __viaddmax_s16x2(left, ng, __vadd2(d, s)); }
+    __device__ static __forceinline__ W cell_chain(W up, W ng, W part) { return __viaddmax_s16x2(up, ng, part); }
 };
 
 // R profile bytes of one lane for residue code b, from the staged strip.
@@ -346,45 +352,259 @@ __global__ void __launch_bounds__(WPB * 32) nw_plain_kernel(NwParams p, uint64_t
     }
 }
 
-// Persistent: one launch over every clean task in cost order (rows longest
-// first); warps take the next task from a global counter.
-template <int R, int WPB>
-__global__ void __launch_bounds__(WPB * 32) nw_persistent_kernel(NwParams p)
+// ---------------------------------------------------------------- batched kernel
+//
+// One persistent launch over every clean pair. The length-sorted sequences
+// are taken two at a time as a rows pair (X1, X2) = (sorted 2k, sorted 2k+1);
+// a task is one rows pair against a group of W consecutive column sequences,
+// one per warp of the CTA. On the 16-bit path the two rows sequences share
+// every 32-bit lane: X1 in the low half, X2 in the high half, against the same
+// column residue, so one staged profile word is already the packed score pair
+// and each lane does two cells per instruction. The profile strip is staged
+// once per CTA and shared by its W warps. Where the 16-bit bound fails the
+// task runs both rows sequences one after the other in 32-bit lanes.
+// CTAs take tasks from a global counter in cost order (longest rows pairs
+// first), so the tail of the launch is the cheapest work.
+
+struct BatchParams {
+    const uint8_t *units;
+    const uint64_t *uoff;
+    const uint32_t *eff;
+    const int8_t *prof;
+    const uint64_t *poff;
+    const uint32_t *plp;
+    const uint32_t *sorted;
+    uint32_t nclean;
+    uint32_t npairs_rows;       // number of rows pairs, ceil(nclean / 2)
+    const uint64_t *row_task;   // first task of each rows pair (npairs_rows + 1)
+    const uint8_t *row_narrow;  // 16-bit tasks for this rows pair
+    uint64_t ntasks;
+    uint32_t *bound;
+    uint64_t bound_stride;
+    int32_t *out;
+    int32_t g;
+    unsigned long long *counter;
+};
+
+namespace dev {
+
+// Stages strip rows [i0, i0 + 32R) as 32-bit profile words in shared memory,
+// laid out [code][plane of 4 rows][lane][4 words] so that one 16-byte load per
+// lane and plane is bank-conflict free for any codes the lanes hold.
+// Narrow: word = (s(X1_i, b), s(X2_i, b)) as int16x2. Wide: word = s(X_i, b).
+template <int R, bool kNarrow>
+__device__ __forceinline__ void stage_words(uint32_t *sprof, const int8_t *__restrict__ g1, uint32_t lp1,
+                                            const int8_t *__restrict__ g2, uint32_t lp2, bool have2, int i0)
 {
-    extern __shared__ __align__(16) int8_t smem[];
+    constexpr int SH = 32 * R;
+    constexpr int CH = SH / 16;
+    for(int c = threadIdx.x; c < kAlpha * CH; c += blockDim.x) {
+        const int b = c / CH, w = c - b * CH;
+        const uint4 va = __ldg(reinterpret_cast<const uint4 *>(g1 + (size_t) b * lp1 + i0) + w);
+        uint4 vb = make_uint4(0, 0, 0, 0);
+        if constexpr(kNarrow) {
+            if(have2) vb = __ldg(reinterpret_cast<const uint4 *>(g2 + (size_t) b * lp2 + i0) + w);
+        }
+        const int ln = w / (R / 16);
+        const int pl0 = (w - ln * (R / 16)) * 4;
+        const uint32_t a4[4] = {va.x, va.y, va.z, va.w};
+        const uint32_t b4[4] = {vb.x, vb.y, vb.z, vb.w};
+#pragma unroll
+        for(int q = 0; q < 4; ++q) {
+            uint4 o;
+            if constexpr(kNarrow) {
+                o.x = sbyte2<0>(a4[q], b4[q]);
+                o.y = sbyte2<1>(a4[q], b4[q]);
+                o.z = sbyte2<2>(a4[q], b4[q]);
+                o.w = sbyte2<3>(a4[q], b4[q]);
+            } else {
+                o.x = (uint32_t) sbyte<0>(a4[q]);
+                o.y = (uint32_t) sbyte<1>(a4[q]);
+                o.z = (uint32_t) sbyte<2>(a4[q]);
+                o.w = (uint32_t) sbyte<3>(a4[q]);
+            }
+            *reinterpret_cast<uint4 *>(sprof + b * SH + (pl0 + q) * 128 + ln * 4) = o;
+        }
+    }
+}
+
+// Sweeps one strip (rows [i0, i0 + 32R)) of one column sequence on the calling
+// warp. `bound` holds the row above the strip on entry (column j at index j)
+// and, when store_bound, the strip's last row on exit. After the call, lane k's
+// H registers hold the strip's rows at the last column.
+template <int R, class K>
+__device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, const uint8_t *__restrict__ cols,
+                                            int ncols, uint32_t *__restrict__ bound, int i0, int tend,
+                                            bool store_bound, int32_t g, int lane, typename K::W (&H)[R])
+{
+    using W = typename K::W;
+    constexpr int SH = 32 * R;
+    const W ng = K::splat(-g);
+#pragma unroll
+    for(int r = 0; r < R; ++r) H[r] = K::splat(-(i0 + lane * R + r + 1) * g);
+    W diag = K::splat(-(i0 + lane * R) * g);
+    W hlast = H[R - 1];
+    uint32_t bq_cur = bound[lane], bq_nxt = bound[32 + lane];
+    const uint32_t *prow = sprof + lane * 4;
+    const bool st31 = store_bound && lane == 31;
+    int j = -lane;
+    uint32_t cur = cols[j], nxt = cols[j + 1];   // columns -32..ncols+34 lie in the padded store
+    const int tend4 = (tend + 3) & ~3;
+    for(int t0 = 0; t0 < tend4; t0 += 4) {
+        if((t0 & 31) == 0 && t0 > 0) {
+            bq_cur = bq_nxt;
+            bq_nxt = bound[t0 + 32 + lane];
+        }
+#pragma unroll
+        for(int u = 0; u < 4; ++u) {
+            W up = __shfl_up_sync(kFull, hlast, 1);
+            const uint32_t bv = __shfl_sync(kFull, bq_cur, (t0 & 31) + u);
+            if(lane == 0) up = (W) bv;
+            if((unsigned) j < (unsigned) ncols) {
+                const uint32_t *pb = prow + cur * SH;
+                uint4 pw = *reinterpret_cast<const uint4 *>(pb);
+                W sc[4] = {(W) pw.x, (W) pw.y, (W) pw.z, (W) pw.w};
+                // Row r needs the old H[r-1] (diagonal) and old H[r] (left): the
+                // off-chain part for row r+1 is computed before row r is
+                // overwritten, so no register copies are needed.
+                W pn = K::cell_part(diag, sc[0], H[0], ng);
+                W u_ = up;
+#pragma unroll
+                for(int r = 0; r < R; ++r) {
+                    const W pr = pn;
+                    if(r + 1 < R) {
+                        if(((r + 1) & 3) == 0) {
+                            pw = *reinterpret_cast<const uint4 *>(pb + ((r + 1) >> 2) * 128);
+                            sc[0] = (W) pw.x; sc[1] = (W) pw.y; sc[2] = (W) pw.z; sc[3] = (W) pw.w;
+                        }
+                        pn = K::cell_part(H[r], sc[(r + 1) & 3], H[r + 1], ng);
+                    }
+                    H[r] = K::cell_chain(u_, ng, pr);
+                    u_ = H[r];
+                }
+                hlast = H[R - 1];
+                if(st31) bound[j] = (uint32_t) hlast;
+                diag = up;
+            }
+            cur = nxt;
+            nxt = cols[j + 2];
+            ++j;
+        }
+    }
+}
+
+template <int R, class K>
+__device__ __forceinline__ typename K::W pick_row(const typename K::W (&H)[R], int r)
+{
+    typename K::W v = H[0];
+#pragma unroll
+    for(int q = 1; q < R; ++q) if(q == r) v = H[q];
+    return v;
+}
+
+}  // namespace dev
+
+template <int R, int W>
+__global__ void __launch_bounds__(W * 32) nw_batched_kernel(BatchParams p)
+{
+    extern __shared__ __align__(16) uint32_t sprof_b[];
+    __shared__ unsigned long long task_q;
+    constexpr int SH = 32 * R;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    int8_t *sprof = smem + warp * (kAlpha * 32 * R);
-    const uint64_t gw = (uint64_t) blockIdx.x * WPB + warp;
-    uint32_t *bound = p.bound + gw * p.bound_stride;
+    uint32_t *bound = p.bound + ((uint64_t) blockIdx.x * W + warp) * p.bound_stride;
+
     for(;;) {
-        unsigned long long q = 0;
-        if(lane == 0) q = atomicAdd(p.counter, 1ull);
-        q = __shfl_sync(dev::kFull, q, 0);
+        __syncthreads();
+        if(threadIdx.x == 0) task_q = atomicAdd(p.counter, 1ull);
+        __syncthreads();
+        const unsigned long long q = task_q;
         if(q >= p.ntasks) break;
-        // Row of task q: binary search over row_task.
-        uint32_t lo = 0, hi = p.nclean - 1;
+        uint32_t lo = 0, hi = p.npairs_rows - 1;
         while(lo < hi) {
             const uint32_t mid = (lo + hi + 1) >> 1;
             if(p.row_task[mid] <= q) lo = mid; else hi = mid - 1;
         }
-        const uint32_t a = lo;
-        const uint64_t t = q - p.row_task[a];
-        const uint32_t ri = p.sorted[a];
-        if(p.row_narrow[a]) {
-            const uint32_t b1 = a + 1 + (uint32_t) (2 * t);
-            const uint32_t b2 = (b1 + 1 < p.nclean) ? b1 + 1 : b1;
-            const uint32_t c1 = p.sorted[b1], c2 = p.sorted[b2];
+        const uint32_t k = lo;
+        const uint32_t grp = (uint32_t) (q - p.row_task[k]);
+        const uint32_t a1 = 2 * k, a2 = min(2 * k + 1, p.nclean - 1);
+        const uint32_t b = 2 * k + 1 + grp * W + warp;
+        const bool has = b < p.nclean;
+        const uint32_t x1 = p.sorted[a1], x2 = p.sorted[a2];
+        const uint32_t y = has ? p.sorted[b] : x1;
+        const int e1 = (int) p.eff[x1], e2 = (int) p.eff[x2];
+        const int ncols = has ? (int) p.eff[y] : 0;
+        const uint8_t *cols = p.units + p.uoff[y];
+        const int8_t *g1 = p.prof + p.poff[x1];
+        const int8_t *g2 = p.prof + p.poff[x2];
+        const uint32_t lp1 = p.plp[x1];
+
+        if(p.row_narrow[k]) {
+            using Wd = dev::Narrow::W;
+            // Row zero of the DP as the boundary above the first strip.
+            if(has) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = dev::dup16(-(jj + 1) * p.g);
+            const int nstrips = (e1 + SH - 1) / SH;
+            const int s2 = (e2 - 1) / SH;
             int32_t r1 = 0, r2 = 0;
-            dev::run_task<R, dev::Narrow, false>(p.prof + p.poff[ri], p.plp[ri], (int) p.eff[ri],
-                                                 p.units + p.uoff[c1], (int) p.eff[c1],
-                                                 p.units + p.uoff[c2], (int) p.eff[c2],
-                                                 sprof, bound, p.g, lane, r1, r2);
-            if(lane == 0) {
-                p.out[dev::tri_index(ri, c1)] = r1;
-                if(b2 != b1) p.out[dev::tri_index(ri, c2)] = r2;
+            for(int s = 0; s < nstrips; ++s) {
+                const int i0 = s * SH;
+                __syncthreads();
+                dev::stage_words<R, true>(sprof_b, g1, lp1, g2, p.plp[x2], (uint32_t) i0 < p.plp[x2], i0);
+                __syncthreads();
+                if(has) {
+                    const bool last = s == nstrips - 1;
+                    const int k1 = last ? (e1 - 1 - i0) / R : 31;
+                    Wd H[R];
+                    __syncwarp();
+                    dev::sweep_strip<R, dev::Narrow>(sprof_b, cols, ncols, bound, i0, ncols + k1, !last, p.g, lane, H);
+                    __syncwarp();
+                    if(s == s2) {
+                        const int rr = e2 - 1 - i0;
+                        const Wd v = dev::pick_row<R, dev::Narrow>(H, rr % R);
+                        const int v2 = __shfl_sync(dev::kFull, dev::hi16(v), rr / R);
+                        r2 = v2;
+                    }
+                    if(last) {
+                        const int rr = e1 - 1 - i0;
+                        const Wd v = dev::pick_row<R, dev::Narrow>(H, rr % R);
+                        r1 = __shfl_sync(dev::kFull, dev::lo16(v), rr / R);
+                    }
+                }
+            }
+            if(has && lane == 0) {
+                p.out[dev::tri_index(x1, y)] = r1;
+                if(b != a2) p.out[dev::tri_index(x2, y)] = r2;
             }
         } else {
-            clean_pair_task<R>(p, a, a + 1 + (uint32_t) t, sprof, bound, lane);
+            using Wd = dev::Wide::W;
+            for(int h = 0; h < 2; ++h) {
+                if(h == 1 && a2 == a1) break;   // CTA-uniform
+                const uint32_t xr = h ? x2 : x1;
+                const int er = h ? e2 : e1;
+                const bool mine = has && !(h == 1 && b == a2);
+                if(mine) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = (uint32_t) (-(jj + 1) * p.g);
+                const int nstrips = (er + SH - 1) / SH;
+                int32_t res = 0;
+                for(int s = 0; s < nstrips; ++s) {
+                    const int i0 = s * SH;
+                    __syncthreads();
+                    dev::stage_words<R, false>(sprof_b, p.prof + p.poff[xr], p.plp[xr], nullptr, 0, false, i0);
+                    __syncthreads();
+                    if(mine) {
+                        const bool last = s == nstrips - 1;
+                        const int k1 = last ? (er - 1 - i0) / R : 31;
+                        Wd H[R];
+                        __syncwarp();
+                        dev::sweep_strip<R, dev::Wide>(sprof_b, cols, ncols, bound, i0, ncols + k1, !last, p.g, lane, H);
+                        __syncwarp();
+                        if(last) {
+                            const int rr = er - 1 - i0;
+                            const Wd v = dev::pick_row<R, dev::Wide>(H, rr % R);
+                            res = __shfl_sync(dev::kFull, v, rr / R);
+                        }
+                    }
+                }
+                if(mine && lane == 0) p.out[dev::tri_index(xr, y)] = res;
+            }
         }
     }
 }
@@ -475,13 +695,39 @@ static int occupancy(KernelT kernel, size_t smem, int *blocks)
     return 0;
 }
 
-// Upper bound on |H| for a task: every path of an (rows_p x cols) DP moves
-// through at most rows_p + cols cells, each changing H by at most
-// max(|score|, g); the extra 2*max covers the d+s intermediate.
-static inline int64_t value_bound(int64_t rows_p, int64_t cols, const ExtTable &t)
+// 16-bit lanes are exact when every value a task can produce fits int16:
+// H(i,j) lies in [-g(i+j), max(smax,0)*min(i,j)] for all i <= rows (padded
+// strip rows included, whose scores are 0) and j <= cols, and the two partial
+// sums (diag + s, left - g) reach at most max(g, |smin|) below the floor.
+static inline bool narrow_ok(int64_t rows_p, int64_t cols, const ExtTable &t)
 {
-    const int64_t m = std::max<int64_t>(t.max_abs, t.penalty);
-    return (rows_p + cols + 2) * m;
+    const int64_t lo = (int64_t) t.penalty * (rows_p + cols) + std::max<int64_t>(t.penalty, t.max_neg);
+    const int64_t hi = (int64_t) std::max<int32_t>(t.max_pos, 0) * std::min(rows_p, cols);
+    return lo <= 32768 && hi <= 32767;
+}
+
+// Batched-kernel tile shapes: rows per lane R and warps per CTA W.
+struct Tiles { int R, W; };
+#include "autotune.inc"
+
+template <int R, int W>
+static int launch_batched(msa_ctx *ctx, const BatchParams &bp0, uint64_t ntasks, uint32_t *launches)
+{
+    BatchParams bp = bp0;
+    auto kern = nw_batched_kernel<R, W>;
+    const size_t smem = (size_t) kAlpha * 32 * R * 4;
+    MSA_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    int bps = 0;
+    MSA_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, W * 32, smem));
+    if(bps < 1) return set_error(ctx, MSA_ERR_CUDA, "batched NW kernel cannot be resident");
+    const uint64_t grid = std::min<uint64_t>((uint64_t) ctx->num_sms * bps, std::max<uint64_t>(ntasks, 1));
+    MSA_CUDA_TRY(ctx, ctx->bound.ensure(grid * W * bp.bound_stride * sizeof(uint32_t)));
+    bp.bound = (uint32_t *) ctx->bound.ptr;
+    kern<<<(unsigned) grid, W * 32, smem, ctx->stream>>>(bp);
+    MSA_CUDA_TRY(ctx, cudaGetLastError());
+    ctx->launches++;
+    (*launches)++;
+    return MSA_OK;
 }
 
 int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d_out)
@@ -544,18 +790,16 @@ int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d
     p.nclean = nclean;
     p.out = d_out;
     p.g = tbl.penalty;
-    p.bound_stride = round_up((uint64_t) max_cols + 96, 32);
+    p.bound_stride = round_up((uint64_t) max_cols + 160, 32);
 
     auto kplain = nw_plain_kernel<kPlainR, kWPB>;
-    auto kpers = nw_persistent_kernel<kPlainR, kWPB>;
     auto kgen = nw_generic_kernel<kPlainR, kWPB>;
     const size_t smem = smem_bytes<kPlainR>();
     int bps = 0;
     if(occupancy(kplain, smem, &bps)) return set_error(ctx, MSA_ERR_CUDA, "occupancy query failed (no sm_100a image?)");
-    int bps2 = 0, bps3 = 0;
-    if(occupancy(kpers, smem, &bps2) || occupancy(kgen, smem, &bps3))
-        return set_error(ctx, MSA_ERR_CUDA, "occupancy query failed");
-    bps = std::min(bps, std::min(bps2, bps3));
+    int bps3 = 0;
+    if(occupancy(kgen, smem, &bps3)) return set_error(ctx, MSA_ERR_CUDA, "occupancy query failed");
+    bps = std::min(bps, bps3);
     const uint64_t resident_blocks = (uint64_t) ctx->num_sms * (uint64_t) bps;
     const uint64_t resident_warps = resident_blocks * kWPB;
 
@@ -597,43 +841,59 @@ int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d
                 a = a2;
             }
         } else {
-            // Tasks per sorted row; 16-bit tasks where the bound allows.
-            std::vector<uint64_t> row_task(nclean + 1, 0);
-            std::vector<uint8_t> row_narrow(nclean, 0);
-            constexpr int SH = 32 * kPlainR;
+            // Rows pairs (sorted 2k, 2k+1) against column groups of W sequences.
+            const Tiles tl = ctx->tile_r ? Tiles{ctx->tile_r, ctx->tile_w} : pick_tiles(st, nclean);
+            const int SH = 32 * tl.R;
+            const uint32_t K = (nclean + 1) / 2;
+            std::vector<uint64_t> row_task(K + 1, 0);
+            std::vector<uint8_t> row_narrow(K, 0);
             uint64_t q = 0;
             uint32_t narrow_tasks = 0;
-            for(uint32_t a = 0; a < nclean; ++a) {
-                row_task[a] = q;
-                const uint64_t cnt = nclean - 1 - a;
-                if(cnt == 0) continue;
-                const int64_t rows_p = (int64_t) round_up(st->eff[st->clean_sorted[a]], SH);
-                const int64_t cols = st->eff[st->clean_sorted[a + 1]];
-                const bool narrow = value_bound(rows_p, cols, tbl) <= 32000;
-                row_narrow[a] = narrow ? 1 : 0;
-                const uint64_t tasks = narrow ? (cnt + 1) / 2 : cnt;
-                if(narrow) narrow_tasks += (uint32_t) tasks;
-                q += tasks;
+            for(uint32_t k = 0; k < K; ++k) {
+                row_task[k] = q;
+                const int64_t ncol = (int64_t) nclean - (2 * (int64_t) k + 1);
+                if(ncol <= 0) continue;
+                const int64_t rows_p = (int64_t) round_up(st->eff[st->clean_sorted[2 * k]], SH);
+                const int64_t cols = st->eff[st->clean_sorted[2 * k + 1]];
+                const bool nar = narrow_ok(rows_p, cols, tbl);
+                row_narrow[k] = nar ? 1 : 0;
+                const uint64_t groups = (uint64_t) (ncol + tl.W - 1) / tl.W;
+                if(nar) narrow_tasks += (uint32_t) groups;
+                q += groups;
             }
-            row_task[nclean] = q;
+            row_task[K] = q;
             stats.narrow_tasks = narrow_tasks;
-            const size_t tb = (nclean + 1) * sizeof(uint64_t) + nclean + 16;
+            const size_t tb = (K + 1) * sizeof(uint64_t) + K + 16;
             MSA_CUDA_TRY(ctx, ctx->tasks.ensure(tb));
             MSA_CUDA_TRY(ctx, ctx->counters.ensure(64));
             uint64_t *d_rt = (uint64_t *) ctx->tasks.ptr;
-            uint8_t *d_rn = (uint8_t *) (d_rt + nclean + 1);
-            MSA_CUDA_TRY(ctx, cudaMemcpyAsync(d_rt, row_task.data(), (nclean + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-            MSA_CUDA_TRY(ctx, cudaMemcpyAsync(d_rn, row_narrow.data(), nclean, cudaMemcpyHostToDevice, s));
+            uint8_t *d_rn = (uint8_t *) (d_rt + K + 1);
+            MSA_CUDA_TRY(ctx, cudaMemcpyAsync(d_rt, row_task.data(), (K + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+            MSA_CUDA_TRY(ctx, cudaMemcpyAsync(d_rn, row_narrow.data(), K, cudaMemcpyHostToDevice, s));
             MSA_CUDA_TRY(ctx, cudaMemsetAsync(ctx->counters.ptr, 0, 64, s));
-            p.row_task = d_rt;
-            p.row_narrow = d_rn;
-            p.ntasks = q;
-            p.counter = (unsigned long long *) ctx->counters.ptr;
-            const uint64_t blocks = std::min<uint64_t>(resident_blocks, (q + kWPB - 1) / kWPB);
-            kpers<<<(unsigned) std::max<uint64_t>(blocks, 1), kWPB * 32, smem, s>>>(p);
-            MSA_CUDA_TRY(ctx, cudaGetLastError());
-            ctx->launches++;
-            stats.launches++;
+            BatchParams bp{};
+            bp.units = st->d_units;
+            bp.uoff = st->d_off;
+            bp.eff = st->d_eff;
+            bp.prof = d_prof;
+            bp.poff = st->d_prof_off;
+            bp.plp = st->d_prof_lp;
+            bp.sorted = st->d_clean_sorted;
+            bp.nclean = nclean;
+            bp.npairs_rows = K;
+            bp.row_task = d_rt;
+            bp.row_narrow = d_rn;
+            bp.ntasks = q;
+            bp.bound_stride = p.bound_stride;
+            bp.out = d_out;
+            bp.g = tbl.penalty;
+            bp.counter = (unsigned long long *) ctx->counters.ptr;
+            int rc = MSA_OK;
+            if(tl.R == 16 && tl.W == 4) rc = launch_batched<16, 4>(ctx, bp, q, &stats.launches);
+            else if(tl.R == 16 && tl.W == 8) rc = launch_batched<16, 8>(ctx, bp, q, &stats.launches);
+            else if(tl.R == 32 && tl.W == 4) rc = launch_batched<32, 4>(ctx, bp, q, &stats.launches);
+            else rc = launch_batched<32, 8>(ctx, bp, q, &stats.launches);
+            if(rc) return rc;
         }
     }
 
@@ -644,10 +904,10 @@ int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d
     cudaEventElapsedTime(&ms_t, ctx->ev[0], ctx->ev[2]);
     stats.kernel_ms = ms_k;
     stats.total_ms = ms_t;
-    uint64_t cells = 0;
-    for(uint32_t i = 1; i < n; ++i)
-        for(uint32_t j = 0; j < i; ++j) cells += st->len[i] * st->len[j];
-    stats.cells = cells;
+    // sum over pairs of L_i * L_j = ((sum L)^2 - sum L^2) / 2, in 128-bit arithmetic.
+    unsigned __int128 s1 = 0, s2 = 0;
+    for(uint32_t i = 0; i < n; ++i) { s1 += st->len[i]; s2 += (unsigned __int128) st->len[i] * st->len[i]; }
+    stats.cells = (uint64_t) ((s1 * s1 - s2) / 2);
     ctx->last = stats;
     return MSA_OK;
 }

@@ -31,7 +31,7 @@ int make_ext_table(const msa_table *t, ExtTable *out, std::string *err)
 {
     std::memset(out, 0, sizeof(*out));
     out->penalty = t->penalty;
-    int32_t mx = 0;
+    int32_t mx = 0, mpos = -128, mneg = 0;
     for(int x = 0; x < kAlpha; ++x) {
         for(int y = 0; y < kAlpha; ++y) {
             int32_t v = 0;
@@ -51,7 +51,11 @@ int make_ext_table(const msa_table *t, ExtTable *out, std::string *err)
             }
             out->valid[x * kAlpha + y] = ok ? 1 : 0;
             out->score[x * kAlpha + y] = (int8_t) v;
-            if(ok && x != MSA_UNIT_END && y != MSA_UNIT_END) mx = std::max(mx, v < 0 ? -v : v);
+            if(ok && x != MSA_UNIT_END && y != MSA_UNIT_END) {
+                mx = std::max(mx, v < 0 ? -v : v);
+                mpos = std::max(mpos, v);
+                if(v < 0) mneg = std::max(mneg, -v);
+            }
         }
     }
     if(t->penalty < 0 || t->penalty > (1 << 20)) {
@@ -59,6 +63,8 @@ int make_ext_table(const msa_table *t, ExtTable *out, std::string *err)
         return MSA_ERR_INVALID;
     }
     out->max_abs = mx;
+    out->max_pos = mpos;
+    out->max_neg = mneg;
     return MSA_OK;
 }
 

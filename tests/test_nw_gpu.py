@@ -145,3 +145,23 @@ def test_stats_and_launch_counts(gpu):
     assert s.pairs == 200 * 199 // 2 and s.cells == wl.cells()
     assert s.launches >= 2 and gpu.launches - before == s.launches
     assert s.narrow_tasks > 0 and s.kernel_ms > 0
+
+
+@pytest.mark.parametrize("tiles", [(16, 4), (16, 8), (32, 4), (32, 8)])
+def test_every_tile_shape_matches_oracle(gpu, tables, tiles):
+    wl = W.random_set(48, 23, 30, 2200, alphabet=b"ARNDCQEGHILKMFPSTWYV")
+    want = oracle_scores(wl, "blosum62", tables)
+    _lib.check(_lib.lib().msa_nw_set_tiles(gpu.handle, *tiles))
+    try:
+        got = gpu_scores(wl, "blosum62", _lib.MSA_NW_PERSISTENT)
+    finally:
+        _lib.lib().msa_nw_set_tiles(gpu.handle, 0, 0)
+    assert np.array_equal(got, want)
+
+
+def test_wide_rows_pairs_match_oracle(gpu, tables):
+    # blosum62 lengths past the 16-bit bound run the rows pair in 32-bit lanes.
+    wl = W.random_set(49, 7, 3000, 4200, alphabet=b"ARNDCQEGHILKMFPSTWYV")
+    got = gpu_scores(wl, "blosum62", _lib.MSA_NW_PERSISTENT)
+    assert np.array_equal(got, oracle_scores(wl, "blosum62", tables))
+    assert pairwise.last_stats().narrow_tasks == 0
