@@ -391,47 +391,45 @@ namespace dev {
 // Stages strip rows [i0, i0 + 32R) as 32-bit profile words in shared memory,
 // laid out [code][plane of 4 rows][lane][4 words] so that one 16-byte load per
 // lane and plane is bank-conflict free for any codes the lanes hold.
-// Narrow: word = (s(X1_i, b), s(X2_i, b)) as int16x2. Wide: word = s(X_i, b).
+// Narrow: word = (s(X1_i, b), s(X2_i, b)) as int16x2; rows of X2 past its
+// profile (lp2) read as 0. Wide: word = s(X1_i, b) as int32.
 template <int R, bool kNarrow>
 __device__ __forceinline__ void stage_words(uint32_t *sprof, const int8_t *__restrict__ g1, uint32_t lp1,
-                                            const int8_t *__restrict__ g2, uint32_t lp2, bool have2, int i0)
+                                            const int8_t *__restrict__ g2, uint32_t lp2, int i0)
 {
     constexpr int SH = 32 * R;
-    constexpr int CH = SH / 16;
-    for(int c = threadIdx.x; c < kAlpha * CH; c += blockDim.x) {
-        const int b = c / CH, w = c - b * CH;
-        const uint4 va = __ldg(reinterpret_cast<const uint4 *>(g1 + (size_t) b * lp1 + i0) + w);
-        uint4 vb = make_uint4(0, 0, 0, 0);
+    constexpr int G = SH / 4;        // 4-row groups per code row
+    constexpr int PL = R / 4;        // planes per lane
+    for(int c = threadIdx.x; c < kAlpha * G; c += blockDim.x) {
+        const int b = c / G, rg = c - b * G;
+        const uint32_t va = __ldg(reinterpret_cast<const uint32_t *>(g1 + (size_t) b * lp1 + i0) + rg);
+        const int ln = rg / PL, pl = rg - ln * PL;
+        uint4 o;
         if constexpr(kNarrow) {
-            if(have2) vb = __ldg(reinterpret_cast<const uint4 *>(g2 + (size_t) b * lp2 + i0) + w);
+            uint32_t vb = 0;
+            if((uint32_t) (i0 + 4 * rg) < lp2) vb = __ldg(reinterpret_cast<const uint32_t *>(g2 + (size_t) b * lp2 + i0) + rg);
+            o.x = sbyte2<0>(va, vb);
+            o.y = sbyte2<1>(va, vb);
+            o.z = sbyte2<2>(va, vb);
+            o.w = sbyte2<3>(va, vb);
+        } else {
+            o.x = (uint32_t) sbyte<0>(va);
+            o.y = (uint32_t) sbyte<1>(va);
+            o.z = (uint32_t) sbyte<2>(va);
+            o.w = (uint32_t) sbyte<3>(va);
         }
-        const int ln = w / (R / 16);
-        const int pl0 = (w - ln * (R / 16)) * 4;
-        const uint32_t a4[4] = {va.x, va.y, va.z, va.w};
-        const uint32_t b4[4] = {vb.x, vb.y, vb.z, vb.w};
-#pragma unroll
-        for(int q = 0; q < 4; ++q) {
-            uint4 o;
-            if constexpr(kNarrow) {
-                o.x = sbyte2<0>(a4[q], b4[q]);
-                o.y = sbyte2<1>(a4[q], b4[q]);
-                o.z = sbyte2<2>(a4[q], b4[q]);
-                o.w = sbyte2<3>(a4[q], b4[q]);
-            } else {
-                o.x = (uint32_t) sbyte<0>(a4[q]);
-                o.y = (uint32_t) sbyte<1>(a4[q]);
-                o.z = (uint32_t) sbyte<2>(a4[q]);
-                o.w = (uint32_t) sbyte<3>(a4[q]);
-            }
-            *reinterpret_cast<uint4 *>(sprof + b * SH + (pl0 + q) * 128 + ln * 4) = o;
-        }
+        *reinterpret_cast<uint4 *>(sprof + b * SH + pl * 128 + ln * 4) = o;
     }
 }
+
+template <bool V> struct Guard { static constexpr bool value = V; };
 
 // Sweeps one strip (rows [i0, i0 + 32R)) of one column sequence on the calling
 // warp. `bound` holds the row above the strip on entry (column j at index j)
 // and, when store_bound, the strip's last row on exit. After the call, lane k's
-// H registers hold the strip's rows at the last column.
+// H registers hold the strip's rows at the last column it reached
+// (tend - 1 - lane). Steps run in groups of 4; only the fill and drain groups,
+// where some lanes sit outside [0, ncols), test the lane's column.
 template <int R, class K>
 __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, const uint8_t *__restrict__ cols,
                                             int ncols, uint32_t *__restrict__ bound, int i0, int tend,
@@ -448,9 +446,10 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
     const uint32_t *prow = sprof + lane * 4;
     const bool st31 = store_bound && lane == 31;
     int j = -lane;
-    uint32_t cur = cols[j], nxt = cols[j + 1];   // columns -32..ncols+34 lie in the padded store
-    const int tend4 = (tend + 3) & ~3;
-    for(int t0 = 0; t0 < tend4; t0 += 4) {
+    uint32_t cur = cols[j], nxt = cols[j + 1];   // columns -32..ncols+35 lie in the padded store
+
+    auto group = [&](int t0, auto guard) {
+        constexpr bool kG = decltype(guard)::value;
         if((t0 & 31) == 0 && t0 > 0) {
             bq_cur = bq_nxt;
             bq_nxt = bound[t0 + 32 + lane];
@@ -460,7 +459,7 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
             W up = __shfl_up_sync(kFull, hlast, 1);
             const uint32_t bv = __shfl_sync(kFull, bq_cur, (t0 & 31) + u);
             if(lane == 0) up = (W) bv;
-            if((unsigned) j < (unsigned) ncols) {
+            if(!kG || (unsigned) j < (unsigned) ncols) {
                 const uint32_t *pb = prow + cur * SH;
                 uint4 pw = *reinterpret_cast<const uint4 *>(pb);
                 W sc[4] = {(W) pw.x, (W) pw.y, (W) pw.z, (W) pw.w};
@@ -490,7 +489,16 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
             nxt = cols[j + 2];
             ++j;
         }
-    }
+    };
+
+    const int tend4 = (tend + 3) & ~3;
+    int t0 = 0;
+#pragma unroll 1
+    for(; t0 < tend4 && t0 < 32; t0 += 4) group(t0, Guard<true>{});
+#pragma unroll 1
+    for(; t0 + 3 < ncols; t0 += 4) group(t0, Guard<false>{});   // every lane inside [0, ncols)
+#pragma unroll 1
+    for(; t0 < tend4; t0 += 4) group(t0, Guard<true>{});
 }
 
 template <int R, class K>
@@ -502,14 +510,85 @@ __device__ __forceinline__ typename K::W pick_row(const typename K::W (&H)[R], i
     return v;
 }
 
+// One task's work for a 16-bit rows pair with strips of 32R rows.
+template <int R>
+__device__ __noinline__ void narrow_task(uint32_t *sprof, const int8_t *g1, uint32_t lp1, const int8_t *g2,
+                                            uint32_t lp2, int e1, int e2, int nst, bool has, const uint8_t *cols,
+                                            int ncols, uint32_t *bound, int32_t g, int lane, int32_t &r1, int32_t &r2)
+{
+    constexpr int SH = 32 * R;
+    const int s2 = (e2 - 1) / SH;
+    for(int s = 0; s < nst; ++s) {
+        const int i0 = s * SH;
+        __syncthreads();
+        stage_words<R, true>(sprof, g1, lp1, g2, lp2, i0);
+        __syncthreads();
+        if(has) {
+            const bool last = s == nst - 1;
+            const int k1 = last ? (e1 - 1 - i0) / R : 31;
+            Narrow::W H[R];
+            __syncwarp();
+            sweep_strip<R, Narrow>(sprof, cols, ncols, bound, i0, ncols + k1, !last, g, lane, H);
+            __syncwarp();
+            if(s == s2) {
+                const int rr = e2 - 1 - i0;
+                r2 = __shfl_sync(kFull, hi16(pick_row<R, Narrow>(H, rr % R)), rr / R);
+            }
+            if(last) {
+                const int rr = e1 - 1 - i0;
+                r1 = __shfl_sync(kFull, lo16(pick_row<R, Narrow>(H, rr % R)), rr / R);
+            }
+        }
+    }
+}
+
+// One rows sequence in 32-bit lanes with strips of 32R rows.
+template <int R>
+__device__ __noinline__ void wide_task(uint32_t *sprof, const int8_t *g1, uint32_t lp1, int e1, int nst,
+                                          bool mine, const uint8_t *cols, int ncols, uint32_t *bound, int32_t g,
+                                          int lane, int32_t &res)
+{
+    constexpr int SH = 32 * R;
+    for(int s = 0; s < nst; ++s) {
+        const int i0 = s * SH;
+        __syncthreads();
+        stage_words<R, false>(sprof, g1, lp1, nullptr, 0, i0);
+        __syncthreads();
+        if(mine) {
+            const bool last = s == nst - 1;
+            const int k1 = last ? (e1 - 1 - i0) / R : 31;
+            Wide::W H[R];
+            __syncwarp();
+            sweep_strip<R, Wide>(sprof, cols, ncols, bound, i0, ncols + k1, !last, g, lane, H);
+            __syncwarp();
+            if(last) {
+                const int rr = e1 - 1 - i0;
+                res = __shfl_sync(kFull, pick_row<R, Wide>(H, rr % R), rr / R);
+            }
+        }
+    }
+}
+
+// Strip plan for `rows` rows with at most 32*RMAX rows per strip: the fewest
+// strips, each of 32R rows with R the smallest multiple of 4 that covers them.
+template <int RMAX>
+__device__ __forceinline__ void strip_plan(int rows, int &nst, int &R)
+{
+    nst = (rows + 32 * RMAX - 1) / (32 * RMAX);
+    R = (rows + 32 * nst - 1) / (32 * nst);
+    R = (R + 3) & ~3;
+}
+
 }  // namespace dev
 
-template <int R, int W>
-__global__ void __launch_bounds__(W * 32) nw_batched_kernel(BatchParams p)
+// Resident CTAs per SM the batched kernel is compiled for (register budget).
+template <int RMAX, int W> struct BatchOcc { static constexpr int value = (RMAX == 32 ? 16 : 24) / W; };
+
+template <int RMAX, int W>
+__global__ void __launch_bounds__(W * 32, BatchOcc<RMAX, W>::value) nw_batched_kernel(BatchParams p)
 {
     extern __shared__ __align__(16) uint32_t sprof_b[];
     __shared__ unsigned long long task_q;
-    constexpr int SH = 32 * R;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint32_t *bound = p.bound + ((uint64_t) blockIdx.x * W + warp) * p.bound_stride;
 
@@ -534,75 +613,40 @@ __global__ void __launch_bounds__(W * 32) nw_batched_kernel(BatchParams p)
         const int e1 = (int) p.eff[x1], e2 = (int) p.eff[x2];
         const int ncols = has ? (int) p.eff[y] : 0;
         const uint8_t *cols = p.units + p.uoff[y];
-        const int8_t *g1 = p.prof + p.poff[x1];
-        const int8_t *g2 = p.prof + p.poff[x2];
-        const uint32_t lp1 = p.plp[x1];
 
         if(p.row_narrow[k]) {
-            using Wd = dev::Narrow::W;
             // Row zero of the DP as the boundary above the first strip.
             if(has) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = dev::dup16(-(jj + 1) * p.g);
-            const int nstrips = (e1 + SH - 1) / SH;
-            const int s2 = (e2 - 1) / SH;
+            int nst, R;
+            dev::strip_plan<RMAX>(e1, nst, R);
             int32_t r1 = 0, r2 = 0;
-            for(int s = 0; s < nstrips; ++s) {
-                const int i0 = s * SH;
-                __syncthreads();
-                dev::stage_words<R, true>(sprof_b, g1, lp1, g2, p.plp[x2], (uint32_t) i0 < p.plp[x2], i0);
-                __syncthreads();
-                if(has) {
-                    const bool last = s == nstrips - 1;
-                    const int k1 = last ? (e1 - 1 - i0) / R : 31;
-                    Wd H[R];
-                    __syncwarp();
-                    dev::sweep_strip<R, dev::Narrow>(sprof_b, cols, ncols, bound, i0, ncols + k1, !last, p.g, lane, H);
-                    __syncwarp();
-                    if(s == s2) {
-                        const int rr = e2 - 1 - i0;
-                        const Wd v = dev::pick_row<R, dev::Narrow>(H, rr % R);
-                        const int v2 = __shfl_sync(dev::kFull, dev::hi16(v), rr / R);
-                        r2 = v2;
+            const int8_t *g1 = p.prof + p.poff[x1], *g2 = p.prof + p.poff[x2];
+            const uint32_t lp1 = p.plp[x1], lp2 = p.plp[x2];
+#define MSA_NARROW(RR) case RR: dev::narrow_task<RR>(sprof_b, g1, lp1, g2, lp2, e1, e2, nst, has, cols, ncols, bound, p.g, lane, r1, r2); break;
+            switch(R) {
+                MSA_NARROW(4) MSA_NARROW(8) MSA_NARROW(12) MSA_NARROW(16)
+                default:
+                    if constexpr(RMAX > 16) {
+                        switch(R) { MSA_NARROW(20) MSA_NARROW(24) MSA_NARROW(28) MSA_NARROW(32) default: break; }
                     }
-                    if(last) {
-                        const int rr = e1 - 1 - i0;
-                        const Wd v = dev::pick_row<R, dev::Narrow>(H, rr % R);
-                        r1 = __shfl_sync(dev::kFull, dev::lo16(v), rr / R);
-                    }
-                }
+                    break;
             }
+#undef MSA_NARROW
             if(has && lane == 0) {
                 p.out[dev::tri_index(x1, y)] = r1;
                 if(b != a2) p.out[dev::tri_index(x2, y)] = r2;
             }
         } else {
-            using Wd = dev::Wide::W;
             for(int h = 0; h < 2; ++h) {
                 if(h == 1 && a2 == a1) break;   // CTA-uniform
                 const uint32_t xr = h ? x2 : x1;
                 const int er = h ? e2 : e1;
                 const bool mine = has && !(h == 1 && b == a2);
                 if(mine) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = (uint32_t) (-(jj + 1) * p.g);
-                const int nstrips = (er + SH - 1) / SH;
                 int32_t res = 0;
-                for(int s = 0; s < nstrips; ++s) {
-                    const int i0 = s * SH;
-                    __syncthreads();
-                    dev::stage_words<R, false>(sprof_b, p.prof + p.poff[xr], p.plp[xr], nullptr, 0, false, i0);
-                    __syncthreads();
-                    if(mine) {
-                        const bool last = s == nstrips - 1;
-                        const int k1 = last ? (er - 1 - i0) / R : 31;
-                        Wd H[R];
-                        __syncwarp();
-                        dev::sweep_strip<R, dev::Wide>(sprof_b, cols, ncols, bound, i0, ncols + k1, !last, p.g, lane, H);
-                        __syncwarp();
-                        if(last) {
-                            const int rr = er - 1 - i0;
-                            const Wd v = dev::pick_row<R, dev::Wide>(H, rr % R);
-                            res = __shfl_sync(dev::kFull, v, rr / R);
-                        }
-                    }
-                }
+                const int nst = (er + 32 * RMAX - 1) / (32 * RMAX);
+                dev::wide_task<RMAX>(sprof_b, p.prof + p.poff[xr], p.plp[xr], er, nst, mine, cols, ncols, bound,
+                                     p.g, lane, res);
                 if(mine && lane == 0) p.out[dev::tri_index(xr, y)] = res;
             }
         }

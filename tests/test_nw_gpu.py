@@ -161,7 +161,7 @@ def test_every_tile_shape_matches_oracle(gpu, tables, tiles):
 
 def test_wide_rows_pairs_match_oracle(gpu, tables):
     # blosum62 lengths past the 16-bit bound run the rows pair in 32-bit lanes.
-    wl = W.random_set(49, 7, 3000, 4200, alphabet=b"ARNDCQEGHILKMFPSTWYV")
+    wl = W.random_set(49, 7, 4200, 5000, alphabet=b"ARNDCQEGHILKMFPSTWYV")
     got = gpu_scores(wl, "blosum62", _lib.MSA_NW_PERSISTENT)
     assert np.array_equal(got, oracle_scores(wl, "blosum62", tables))
     assert pairwise.last_stats().narrow_tasks == 0
