@@ -337,9 +337,11 @@ def main():
     if rank == 0:
         props = torch.cuda.get_device_properties(local)
         sm_mhz = clocks.get("sm_mhz") or 1965.0
-        # INT32 issue roofline: 4 SM sub-partitions x 32 lanes issue per clock;
-        # 4 algorithmic lane-ops per cell (d+s, max(up,left), -g, max).
-        peak = props.multi_processor_count * 128 * sm_mhz * 1e6 / 4 / 1e9
+        # Integer-issue roofline: max-plus needs two max operations per cell and
+        # every max form (DPX included) issues on the ALU pipe, 64 lanes/clk/SM
+        # (measured by `bench.py --probe`): 32 cells/clk/SM in 32-bit lanes,
+        # 64 in 16x2 lanes.
+        peak = props.multi_processor_count * 64 * sm_mhz * 1e6 / 2 / 1e9
         traffic = None
         tp = ROOT / "profiles" / "nw_traffic.json"
         if tp.exists():
@@ -364,9 +366,10 @@ def main():
                     "d2h_bytes_per_step": int(npairs * 4), "scores_match": e2e_ok},
             "gpu_launches": int(launches),
             "roofline": {"bound": "int32-issue", "achieved": kernel_gcups, "peak": peak, "unit": "GCUPS",
-                         "frac": kernel_gcups / peak, "traffic": traffic,
-                         "peak_basis": f"{props.multi_processor_count} SM x 128 lanes/clk x {sm_mhz:.0f} MHz "
-                                       f"(median sampled) / 4 INT32 ops per cell"},
+                         "frac": kernel_gcups / peak, "frac_x2": kernel_gcups / (2 * peak), "traffic": traffic,
+                         "peak_basis": f"{props.multi_processor_count} SM x 64 ALU lanes/clk x {sm_mhz:.0f} MHz "
+                                       f"(median sampled) / 2 max-ops per cell (int32 lanes); frac_x2 is against "
+                                       f"the 16x2-lane ceiling, twice that"},
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
