@@ -163,6 +163,28 @@ typedef struct msa_nw_stats {
 } msa_nw_stats;
 int msa_nw_last_stats(const msa_ctx *ctx, msa_nw_stats *out);
 
+/*
+ * All-pairs NW that allocates nothing (no counterpart in the reference, which
+ * always allocates per call). For callers that may not call cudaMalloc when
+ * they score, e.g. a runtime that owns all device memory in its own pool, or
+ * code that must avoid the device synchronisation an allocation can imply.
+ * `units` (device) holds the sequences; `offs` and `lens` (host, n entries)
+ * locate sequence k at units[offs[k] .. offs[k]+lens[k]); `out` (device) gets
+ * n(n-1)/2 int32 scores at i(i-1)/2+j, equal to msa_nw_all_pairs. Runs on
+ * `stream` (a cudaStream_t, NULL = legacy default) of the current device and
+ * returns after the scores are written.
+ * Scratch is one fixed 16 MiB device array inside this library, shared by all
+ * calls on a device and keeping the last call's contents: calls that overlap
+ * on the GPU race and must be serialised by the caller. The first call on a
+ * device looks up that array's address, so make it before any stream capture.
+ * Limits: n <= 65536 and sequences up to about one million units; larger
+ * requests return MSA_ERR_TOO_LARGE. msa_noalloc_last_error() explains a
+ * failure.
+ */
+int msa_nw_all_pairs_noalloc(const uint8_t *units, const uint64_t *offs, const uint64_t *lens,
+                             uint32_t n, const msa_table *table, int32_t *out, void *stream);
+const char *msa_noalloc_last_error(void);
+
 /* ---------------------------------------------------------- neighbor-joining */
 
 /* One node of the guide tree: otu + hierarchy

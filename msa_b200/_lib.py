@@ -106,6 +106,9 @@ _PROTOS = [
     ("msa_nw_all_pairs", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(MsaTable), ctypes.c_int,
                                         ctypes.c_void_p, ctypes.c_int]),
     ("msa_nw_set_tiles", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    ("msa_nw_all_pairs_noalloc", ctypes.c_int, [ctypes.c_void_p, c_u64p, c_u64p, ctypes.c_uint32,
+                                                ctypes.POINTER(MsaTable), ctypes.c_void_p, ctypes.c_void_p]),
+    ("msa_noalloc_last_error", ctypes.c_char_p, []),
     ("msa_nw_last_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(MsaNwStats)]),
     ("msa_nj", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32,
                               ctypes.POINTER(MsaOtu)]),
