@@ -192,6 +192,21 @@ def profile_run(args):
     if args.n:
         wl.seqs = wl.seqs[:args.n]
     flat, offs, lens = wl.flat_units()
+    if args.profile == "nj":
+        from msa_b200 import phylogeny
+        tri = pairwise.score_units(flat, offs, lens, ScoringTable(wl.table))
+        times = []
+        for _ in range(args.warmup + 1):
+            t0 = time.perf_counter()
+            phylogeny.run_triangle(tri, wl.n)
+            times.append((time.perf_counter() - t0) * 1e3)
+        import ctypes
+        from msa_b200 import runtime
+        ns = _lib.MsaNjStats()
+        _lib.lib().msa_nj_last_stats(runtime.context(0).handle, ctypes.byref(ns))
+        stats = {f: getattr(ns, f) for f, _ in ns._fields_}
+        print(json.dumps({"workload": args.workload, "n": wl.n, "mode": "nj", "wall_ms": times, "stats": stats}))
+        return
     mode = _lib.MSA_NW_PERSISTENT if args.profile == "persistent" else _lib.MSA_NW_PLAIN
     for _ in range(args.warmup + 1):
         pairwise.score_units(flat, offs, lens, ScoringTable(wl.table), mode)
@@ -211,7 +226,7 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--cpu-cells", type=float, default=1.5e10)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--profile", choices=["persistent", "plain"], default=None,
+    ap.add_argument("--profile", choices=["persistent", "plain", "nj"], default=None,
                     help="profiling run: --warmup calls then one call, on the first --n sequences")
     ap.add_argument("--n", type=int, default=0, help="with --profile: use the first N sequences")
     ap.add_argument("--probe", action="store_true", help="integer-op throughput probes (lane-ops/clk/SM)")
@@ -237,7 +252,8 @@ def main():
     from msa_b200 import ScoringTable, _lib, runtime
     lib = _lib.lib()
     ctx = runtime.context(local)
-    stream = torch.cuda.current_stream()
+    stream = torch.cuda.Stream()          # a capturable stream: repeated calls replay a CUDA graph
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
 
     wl = load_workload(args.workload, rank)
@@ -358,7 +374,7 @@ def main():
             "vs_baseline": None, "dtype": "int32/int16x2", "data": "synthetic (seeded)",
             "config": dict(cfg, parallelism=f"{world} independent replicas (weak)" if world > 1 else "1 GPU",
                            l2="flushed (256 MB write) before every timed step"),
-            "kernel_gcups": kernel_gcups, "narrow_tasks": int(st.narrow_tasks),
+            "kernel_gcups": kernel_gcups, "narrow_tasks": int(st.narrow_tasks), "graph_replay": bool(st.graph),
             "plain": {"value": plain_gcups, "ms_per_step": plain_step, "steps": args.plain_steps,
                       "speedup_persistent_vs_plain": value / plain_gcups, "bit_identical": agree},
             "e2e": {"value": e2e_gcups, "unit": "GCUPS", "ms_per_step": e2e_step,

@@ -160,6 +160,7 @@ typedef struct msa_nw_stats {
     uint64_t pairs;
     uint32_t launches;      /* kernel launches issued by the call */
     uint32_t narrow_tasks;  /* tasks run on 16-bit lanes */
+    uint32_t graph;         /* 1 if the call replayed a captured CUDA graph */
 } msa_nw_stats;
 int msa_nw_last_stats(const msa_ctx *ctx, msa_nw_stats *out);
 
@@ -215,6 +216,19 @@ typedef enum msa_tri_kind {
  * n < 2 writes nothing (phylogeny returns an empty tree).
  */
 int msa_nj(msa_ctx *ctx, const void *tri, int tri_kind, uint32_t n, msa_otu *out_nodes);
+
+/* Timing of the context's last msa_nj call. Cycle counts are block 0's SM
+ * clock cycles by phase: while the whole grid joins (scan, barrier waits,
+ * join) and once one block finishes alone (scan, join). */
+typedef struct msa_nj_stats {
+    double kernel_ms;
+    double total_ms;            /* upload, matrix set-up, joins, download */
+    uint32_t n;
+    uint32_t grid_joins;
+    uint64_t cycles_scan, cycles_wait, cycles_join;
+    uint64_t cycles_scan_single, cycles_join_single;
+} msa_nj_stats;
+int msa_nj_last_stats(const msa_ctx *ctx, msa_nj_stats *out);
 
 /* ------------------------------------------------------------ diagnostics */
 

@@ -51,12 +51,20 @@ class MsaTable(ctypes.Structure):
 
 class MsaNwStats(ctypes.Structure):
     _fields_ = [("kernel_ms", ctypes.c_double), ("total_ms", ctypes.c_double), ("cells", ctypes.c_uint64),
-                ("pairs", ctypes.c_uint64), ("launches", ctypes.c_uint32), ("narrow_tasks", ctypes.c_uint32)]
+                ("pairs", ctypes.c_uint64), ("launches", ctypes.c_uint32), ("narrow_tasks", ctypes.c_uint32),
+                ("graph", ctypes.c_uint32)]
 
 
 class MsaOtu(ctypes.Structure):
     _fields_ = [("parent", ctypes.c_uint32), ("child", ctypes.c_uint32 * 2), ("distance", ctypes.c_float),
                 ("level", ctypes.c_uint32)]
+
+
+class MsaNjStats(ctypes.Structure):
+    _fields_ = [("kernel_ms", ctypes.c_double), ("total_ms", ctypes.c_double), ("n", ctypes.c_uint32),
+                ("grid_joins", ctypes.c_uint32), ("cycles_scan", ctypes.c_uint64), ("cycles_wait", ctypes.c_uint64),
+                ("cycles_join", ctypes.c_uint64), ("cycles_scan_single", ctypes.c_uint64),
+                ("cycles_join_single", ctypes.c_uint64)]
 
 
 class MsaServeConfig(ctypes.Structure):
@@ -112,6 +120,7 @@ _PROTOS = [
     ("msa_nw_last_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(MsaNwStats)]),
     ("msa_nj", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32,
                               ctypes.POINTER(MsaOtu)]),
+    ("msa_nj_last_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(MsaNjStats)]),
     ("msa_probe_op", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(MsaOpProbe)]),
     ("msa_serve_start", ctypes.c_int, [ctypes.POINTER(MsaServeConfig), ctypes.POINTER(ctypes.c_void_p)]),
     ("msa_serve_submit", ctypes.c_int, [ctypes.c_void_p, c_u8p, c_u64p, c_u64p, ctypes.c_uint32,

@@ -2,6 +2,7 @@
 // the all-pairs NW / NJ entry points. Every entry point catches everything
 // and returns a status; nothing throws across the boundary.
 #include <algorithm>
+#include <atomic>
 #include <cstring>
 #include <new>
 #include <numeric>
@@ -54,8 +55,6 @@ static void free_store(SeqStore *st)
     cudaFree(st->d_prof_lp);
     delete st;
 }
-
-void release_graphs(msa_ctx *ctx);
 
 }  // namespace msa
 
@@ -213,6 +212,8 @@ int msa_seqs_upload(msa_ctx *ctx, const uint8_t *units, const uint64_t *offs, co
         if(!e && n) e = cudaMemcpyAsync(st->d_prof_lp, st->prof_lp.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, s);
         if(!e) e = cudaStreamSynchronize(s);   // host staging buffer goes out of scope
         if(e) { free_store(st); return cuda_error(ctx, e, "sequence upload"); }
+        static std::atomic<uint64_t> serials{1};
+        st->serial = serials++;
         const uint64_t h = ctx->next_handle++;
         ctx->stores[h] = st;
         *out = h;
@@ -233,6 +234,7 @@ int msa_seqs_release(msa_ctx *ctx, msa_seqs seqs)
     if(it == ctx->stores.end()) return MSA_ERR_HANDLE;
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    drop_plans_for_store(ctx, it->second->serial);
     free_store(it->second);
     ctx->stores.erase(it);
     return MSA_OK;
@@ -335,6 +337,13 @@ int msa_nw_last_stats(const msa_ctx *ctx, msa_nw_stats *out)
     return MSA_OK;
 }
 
+int msa_nj_last_stats(const msa_ctx *ctx, msa_nj_stats *out)
+{
+    if(!ctx || !out) return MSA_ERR_INVALID;
+    *out = ctx->nj_last;
+    return MSA_OK;
+}
+
 int msa_nj(msa_ctx *ctx, const void *tri, int tri_kind, uint32_t n, msa_otu *out_nodes)
 {
     if(!ctx) return MSA_ERR_INVALID;
@@ -352,7 +361,3 @@ int msa_nj(msa_ctx *ctx, const void *tri, int tri_kind, uint32_t n, msa_otu *out
 }
 
 }  // extern "C"
-
-namespace msa {
-void release_graphs(msa_ctx *) {}
-}

@@ -48,6 +48,7 @@ int make_ext_table(const msa_table *t, ExtTable *out, std::string *err);
 // Device-resident sequence store.
 struct SeqStore {
     uint32_t n = 0;
+    uint64_t serial = 0;            // unique per upload (plans are keyed by it)
     std::vector<uint64_t> len;      // given length (units)
     std::vector<uint32_t> eff;      // index of first END unit within the padded length
     std::vector<uint32_t> plen;     // 3 * ceil(len / 3)
@@ -96,6 +97,7 @@ struct msa_ctx {
     msa::DevBuf prof, bound, tasks, counters, out_tmp, pairs, nj_buf;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     msa_nw_stats last{};
+    msa_nj_stats nj_last{};
     msa::GraphCache *graphs = nullptr;
     int tile_r = 0, tile_w = 0;   // persistent-kernel tile override (0 = autotuned)
 };
@@ -109,6 +111,8 @@ int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d
 constexpr int kUnitFront = 64;
 int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out);
 
+void release_graphs(msa_ctx *ctx);
+void drop_plans_for_store(msa_ctx *ctx, uint64_t serial);
 int set_error(msa_ctx *ctx, int status, const std::string &msg);
 int cuda_error(msa_ctx *ctx, cudaError_t e, const char *what);
 

@@ -72,6 +72,7 @@ struct State {
     float *rec_dx, *rec_dy;
     unsigned *bar;
     int *err;
+    unsigned long long *cycles;   // 6 phase counters written by block 0
     uint32_t n;
     uint32_t single_c;       // block 0 continues alone once c <= single_c
 };
@@ -91,7 +92,7 @@ __device__ __forceinline__ bool grid_sync(unsigned *bar, unsigned nblocks, unsig
             if(v >= target) break;
             if(*(volatile int *) err) break;
             if(++spins > kSpinLimit) { atomicExch(err, 1); break; }
-            __nanosleep(64);
+            __nanosleep(20);
         }
         __threadfence();
     }
@@ -109,13 +110,37 @@ __device__ __forceinline__ void tri_decode(uint64_t L, uint32_t &i, uint32_t &j)
     j = (uint32_t) (L - r * (r - 1) / 2);
 }
 
+// Best (Q, row-major index) of rows gw, gw + nwt, ... of the logical lower
+// triangle. kCG: other blocks write D, so loads bypass L1.
+template <bool kCG>
+__device__ __forceinline__ void scan_rows(const float *__restrict__ D, uint32_t n, const uint32_t *pl, const float *Sl,
+                                          uint32_t c, float cm2, uint32_t gw, uint32_t nwt, int lane, float &bq,
+                                          uint32_t &bl)
+{
+    for(uint32_t i = 1 + gw; i < c; i += nwt) {
+        const float *row = D + (size_t) pl[i] * n;
+        const float si = Sl[i];
+        const uint32_t base = i * (i - 1) / 2;
+        for(uint32_t j = lane; j < i; j += 32) {
+            const float d = kCG ? __ldcg(row + pl[j]) : row[pl[j]];
+            const float q = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d), si), Sl[j]);
+            if(q > bq) { bq = q; bl = base + j; }
+        }
+    }
+}
+
 __global__ void __launch_bounds__(kThreads) nj_kernel(State st)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const uint32_t n = st.n;
-    uint32_t *pl = reinterpret_cast<uint32_t *>(smem_raw);          // logical -> physical
-    float *Sl = reinterpret_cast<float *>(pl + n);                  // S in logical order
-    double *upd = reinterpret_cast<double *>(smem_raw + (size_t) n * 8);   // block 0 update scratch (8-aligned)
+    // Shared layout (16-byte aligned regions): logical -> physical slots, S in
+    // logical order (reused for the float row-sum updates once a join has read
+    // it), and block 0's double-precision updates.
+    const size_t off_s = ((size_t) n * 4 + 15) & ~(size_t) 15;
+    const size_t off_u = (off_s + (size_t) n * 4 + 15) & ~(size_t) 15;
+    uint32_t *pl = reinterpret_cast<uint32_t *>(smem_raw);
+    float *Sl = reinterpret_cast<float *>(smem_raw + off_s);
+    double *upd = reinterpret_cast<double *>(smem_raw + off_u);
     __shared__ unsigned long long wbest[kThreads / 32];
     __shared__ unsigned long long chosen;
     __shared__ uint8_t exact_all;
@@ -123,6 +148,15 @@ __global__ void __launch_bounds__(kThreads) nj_kernel(State st)
     const unsigned nblocks = gridDim.x;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     unsigned epoch = 0;
+    // Block 0, thread 0: cycles spent per phase (grid: scan, wait, join, wait;
+    // single: scan, join) for msa_nj_last_stats.
+    unsigned long long cyc[6] = {0, 0, 0, 0, 0, 0};
+    unsigned long long t_last = clock64();
+    auto mark = [&](int k) {
+        const unsigned long long t = clock64();
+        cyc[k] += t - t_last;
+        t_last = t;
+    };
     uint32_t c = n;
     int buf = 0;
     uint32_t next_parent = n;
@@ -140,29 +174,18 @@ __global__ void __launch_bounds__(kThreads) nj_kernel(State st)
         }
         __syncthreads();
 
-        // ---- scan: this block's slice of the c(c-1)/2 logical pairs.
-        const uint64_t total = (uint64_t) c * (c - 1) / 2;
-        const unsigned nb = single ? 1u : nblocks;
-        const unsigned bid = single ? 0u : blockIdx.x;
-        const uint64_t lo = total * bid / nb, hi = total * (bid + 1) / nb;
+        // ---- scan: warps take rows i = 1..c-1 round-robin; lanes stride over
+        // j < i. Each thread visits its pairs in increasing row-major index, so
+        // a strict `>` keeps its first maximum, as the reference's scan does.
         const float cm2 = (float) (c - 2);
-        unsigned long long best = 0;
-        uint64_t L = lo + tid;
-        if(L < hi) {
-            uint32_t i, j;
-            tri_decode(L, i, j);
-            while(L < hi) {
-                const uint32_t pi = pl[i];
-                const float d = __ldcg(st.D + (size_t) pi * n + pl[j]);
-                float q = __fmul_rn(cm2, d);
-                q = __fsub_rn(q, Sl[i]);
-                q = __fsub_rn(q, Sl[j]);
-                best = umax64(best, pack(order_key(q), (uint32_t) L));
-                L += kThreads;
-                j += kThreads;
-                while(j >= i) { j -= i; ++i; }
-            }
-        }
+        const uint32_t nwt = (single ? 1u : nblocks) * (kThreads / 32);
+        const uint32_t gw = (single ? 0u : blockIdx.x) * (kThreads / 32) + warp;
+        float bq = -INFINITY;
+        uint32_t bl = 0;
+        if(single) scan_rows<false>(st.D, n, pl, Sl, c, cm2, gw, nwt, lane, bq, bl);
+        else scan_rows<true>(st.D, n, pl, Sl, c, cm2, gw, nwt, lane, bq, bl);
+        unsigned long long best = pack(order_key(bq), bl);
+        if(blockIdx.x == 0 && tid == 0) mark(single ? 4 : 0);
         best = warp_max(best);
         if(lane == 0) wbest[warp] = best;
         __syncthreads();
@@ -176,6 +199,7 @@ __global__ void __launch_bounds__(kThreads) nj_kernel(State st)
         }
         if(!single) {
             if(!grid_sync(st.bar, nblocks, epoch, st.err)) return;
+            if(blockIdx.x == 0 && tid == 0) mark(1);
             if(warp == 0) {
                 unsigned long long v = 0;
                 for(unsigned b = lane; b < nblocks; b += 32) v = umax64(v, __ldcg(st.partial + b));
@@ -237,6 +261,7 @@ __global__ void __launch_bounds__(kThreads) nj_kernel(State st)
                     const float s = __double2float_rn(__dadd_rn((double) Sl[i], __dsub_rn(u, (double) prev)));
                     __stcg(st.S + p, s);
                 }
+                Sl[i] = nd;   // this thread's own slot: S[i] was read just above
             }
             if(!exact) exact_all = 0;
             __syncthreads();
@@ -248,7 +273,21 @@ __global__ void __launch_bounds__(kThreads) nj_kernel(State st)
             if(tid == 0) {
                 float ns = 0.0f;
                 if(exact_all) {
-                    for(uint32_t i = 0; i < c; ++i) ns = __fadd_rn(ns, __double2float_rn(upd[i]));
+                    // Prefetched float4 batches keep the loads off the add chain.
+                    const float4 *v4 = reinterpret_cast<const float4 *>(Sl);
+                    const uint32_t c4 = c / 4;
+                    float4 a = c4 > 0 ? v4[0] : make_float4(0, 0, 0, 0);
+                    float4 b = c4 > 1 ? v4[1] : make_float4(0, 0, 0, 0);
+                    for(uint32_t q = 0; q < c4; ++q) {
+                        const float4 cur = a;
+                        a = b;
+                        if(q + 2 < c4) b = v4[q + 2];
+                        ns = __fadd_rn(ns, cur.x);
+                        ns = __fadd_rn(ns, cur.y);
+                        ns = __fadd_rn(ns, cur.z);
+                        ns = __fadd_rn(ns, cur.w);
+                    }
+                    for(uint32_t i = 4 * c4; i < c; ++i) ns = __fadd_rn(ns, Sl[i]);
                 } else {
                     for(uint32_t i = 0; i < c; ++i) ns = __double2float_rn(__dadd_rn((double) ns, upd[i]));
                 }
@@ -268,13 +307,17 @@ __global__ void __launch_bounds__(kThreads) nj_kernel(State st)
         ++step;
         buf ^= 1;
         --c;
+        if(blockIdx.x == 0 && tid == 0) mark(single ? 5 : 2);
         if(!single) {
             if(!grid_sync(st.bar, nblocks, epoch, st.err)) return;
+            if(blockIdx.x == 0 && tid == 0) mark(3);
         } else {
             __threadfence_block();
             __syncthreads();
         }
     }
+    if(blockIdx.x == 0 && tid == 0)
+        for(int k = 0; k < 6; ++k) st.cycles[k] = cyc[k];
 }
 
 // Packed triangle (float or int32) -> full symmetric matrix, diagonal 0.
@@ -311,7 +354,7 @@ __global__ void row_sums_kernel(const float *__restrict__ D, float *__restrict__
 int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out)
 {
     cudaStream_t s = ctx->stream;
-    const size_t smem = (size_t) n * 16;   // pl, Sl (4 B each), upd (8 B)
+    const size_t smem = (size_t) n * 16 + 32;   // pl, Sl (4 B each), upd (8 B), alignment
     if(smem > 200 * 1024) return set_error(ctx, MSA_ERR_TOO_LARGE, "neighbor-joining supports at most 12800 OTUs");
     const uint64_t ntri = (uint64_t) n * (n - 1) / 2;
 
@@ -320,7 +363,7 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out)
     auto take = [&off](size_t b) { size_t o = off; off = round_up(off + b, 256); return o; };
     const size_t oD = take((size_t) n * n * 4), oS = take(n * 4), oP0 = take(n * 4), oP1 = take(n * 4),
                  oM = take(n * 4), oPart = take(4096 * 8), oRx = take(n * 4), oRy = take(n * 4),
-                 oRdx = take(n * 4), oRdy = take(n * 4), oBar = take(64), oErr = take(64),
+                 oRdx = take(n * 4), oRdy = take(n * 4), oBar = take(64), oErr = take(64), oCyc = take(64),
                  oTri = take((kind == MSA_TRI_F32_HOST || kind == MSA_TRI_I32_HOST) ? ntri * 4 : 0);
     MSA_CUDA_TRY(ctx, ctx->nj_buf.ensure(off));
     char *base = (char *) ctx->nj_buf.ptr;
@@ -337,8 +380,10 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out)
     st.rec_dy = (float *) (base + oRdy);
     st.bar = (unsigned *) (base + oBar);
     st.err = (int *) (base + oErr);
+    st.cycles = (unsigned long long *) (base + oCyc);
     st.n = n;
 
+    MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[0], s));
     const void *dtri = tri;
     if(kind == MSA_TRI_F32_HOST || kind == MSA_TRI_I32_HOST) {
         MSA_CUDA_TRY(ctx, cudaMemcpyAsync(base + oTri, tri, ntri * 4, cudaMemcpyHostToDevice, s));
@@ -365,9 +410,12 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out)
     st.single_c = 1024;
     if(n <= st.single_c) grid = 1;
     void *args[] = {&st};
+    MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[1], s));
     MSA_CUDA_TRY(ctx, cudaLaunchCooperativeKernel((const void *) njdev::nj_kernel, dim3(grid), dim3(njdev::kThreads),
                                                   args, smem, s));
+    MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[2], s));
     ctx->launches++;
+    unsigned long long cyc[6] = {0, 0, 0, 0, 0, 0};
 
     std::vector<uint32_t> rx(n - 1), ry(n - 1);
     std::vector<float> rdx(n - 1), rdy(n - 1);
@@ -377,7 +425,24 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out)
     MSA_CUDA_TRY(ctx, cudaMemcpyAsync(rdx.data(), st.rec_dx, (n - 1) * 4, cudaMemcpyDeviceToHost, s));
     MSA_CUDA_TRY(ctx, cudaMemcpyAsync(rdy.data(), st.rec_dy, (n - 1) * 4, cudaMemcpyDeviceToHost, s));
     MSA_CUDA_TRY(ctx, cudaMemcpyAsync(&err, st.err, 4, cudaMemcpyDeviceToHost, s));
+    MSA_CUDA_TRY(ctx, cudaMemcpyAsync(cyc, st.cycles, sizeof(cyc), cudaMemcpyDeviceToHost, s));
     MSA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    {
+        msa_nj_stats ns{};
+        float ms = 0, ms_all = 0;
+        cudaEventElapsedTime(&ms, ctx->ev[1], ctx->ev[2]);
+        cudaEventElapsedTime(&ms_all, ctx->ev[0], ctx->ev[2]);
+        ns.kernel_ms = ms;
+        ns.total_ms = ms_all;
+        ns.n = n;
+        ns.grid_joins = n > st.single_c ? n - st.single_c : 0;
+        ns.cycles_scan = cyc[0];
+        ns.cycles_wait = cyc[1] + cyc[3];
+        ns.cycles_join = cyc[2];
+        ns.cycles_scan_single = cyc[4];
+        ns.cycles_join_single = cyc[5];
+        ctx->nj_last = ns;
+    }
     if(err == 1) return set_error(ctx, MSA_ERR_DEVICE_TIMEOUT, "neighbor-joining grid barrier timed out");
     if(err == 2) return set_error(ctx, MSA_ERR_UNDEFINED, "no joinable pair: every Q value is NaN");
 

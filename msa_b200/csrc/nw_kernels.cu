@@ -754,24 +754,284 @@ static inline bool narrow_ok(int64_t rows_p, int64_t cols, const ExtTable &t)
 struct Tiles { int R, W; };
 #include "autotune.inc"
 
-template <int R, int W>
-static int launch_batched(msa_ctx *ctx, const BatchParams &bp0, uint64_t ntasks, uint32_t *launches)
+
+// ---------------------------------------------------------------- plans and graphs
+//
+// A plan is everything a call needs besides the store: the host-side task
+// tables, and device buffers it owns (score profiles, the table, boundary
+// rows, task tables, the work counter). Plans are cached per context, keyed by
+// store, table, mode, tile shape and output pointer; for the persistent mode
+// the launch sequence is captured once into a CUDA graph and replayed.
+
+struct PlainLaunch { uint64_t k_lo, k_hi, blocks; };
+
+struct NwPlan {
+    uint64_t store_serial = 0;
+    int mode = 0;
+    int32_t *d_out = nullptr;
+    Tiles tiles{0, 0};
+    ExtTable tbl{};
+    DevBuf mem;
+    const int8_t *d_ext = nullptr;
+    NwParams p{};
+    BatchParams bp{};
+    uint32_t n = 0;
+    uint64_t ngeneric = 0, gen_blocks = 0;
+    std::vector<PlainLaunch> plain;
+    uint64_t batch_grid = 0;
+    uint32_t launches = 0, narrow_tasks = 0;
+    uint64_t cells = 0, pairs = 0;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t captured_on = nullptr;
+    ~NwPlan()
+    {
+        if(exec) cudaGraphExecDestroy(exec);
+        mem.release();
+    }
+};
+
+struct GraphCache {
+    std::vector<NwPlan *> plans;   // most recent last
+};
+
+static constexpr size_t kMaxPlans = 2;
+
+void release_graphs(msa_ctx *ctx)
 {
-    BatchParams bp = bp0;
+    if(!ctx->graphs) return;
+    for(NwPlan *pl : ctx->graphs->plans) delete pl;
+    delete ctx->graphs;
+    ctx->graphs = nullptr;
+}
+
+void drop_plans_for_store(msa_ctx *ctx, uint64_t serial)
+{
+    if(!ctx->graphs) return;
+    auto &v = ctx->graphs->plans;
+    for(size_t i = 0; i < v.size();) {
+        if(v[i]->store_serial == serial) { delete v[i]; v.erase(v.begin() + i); }
+        else ++i;
+    }
+}
+
+template <int R, int W>
+static int batched_grid(msa_ctx *ctx, uint64_t ntasks, uint64_t *grid)
+{
     auto kern = nw_batched_kernel<R, W>;
     const size_t smem = (size_t) kAlpha * 32 * R * 4;
     MSA_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     int bps = 0;
     MSA_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, W * 32, smem));
     if(bps < 1) return set_error(ctx, MSA_ERR_CUDA, "batched NW kernel cannot be resident");
-    const uint64_t grid = std::min<uint64_t>((uint64_t) ctx->num_sms * bps, std::max<uint64_t>(ntasks, 1));
-    MSA_CUDA_TRY(ctx, ctx->bound.ensure(grid * W * bp.bound_stride * sizeof(uint32_t)));
-    bp.bound = (uint32_t *) ctx->bound.ptr;
-    kern<<<(unsigned) grid, W * 32, smem, ctx->stream>>>(bp);
-    MSA_CUDA_TRY(ctx, cudaGetLastError());
-    ctx->launches++;
-    (*launches)++;
+    *grid = std::min<uint64_t>((uint64_t) ctx->num_sms * bps, std::max<uint64_t>(ntasks, 1));
     return MSA_OK;
+}
+
+template <int R, int W>
+static void launch_batched(const NwPlan &pl, cudaStream_t s)
+{
+    const size_t smem = (size_t) kAlpha * 32 * R * 4;
+    nw_batched_kernel<R, W><<<(unsigned) pl.batch_grid, W * 32, smem, s>>>(pl.bp);
+}
+
+static int build_plan(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d_out, Tiles tiles,
+                      NwPlan *pl)
+{
+    const uint32_t n = st->n;
+    pl->store_serial = st->serial;
+    pl->mode = mode;
+    pl->d_out = d_out;
+    pl->tiles = tiles;
+    pl->tbl = tbl;
+    pl->n = n;
+    pl->pairs = (uint64_t) n * (n - 1) / 2;
+    // sum over pairs of L_i * L_j = ((sum L)^2 - sum L^2) / 2, in 128-bit arithmetic.
+    unsigned __int128 s1 = 0, s2 = 0;
+    for(uint32_t i = 0; i < n; ++i) { s1 += st->len[i]; s2 += (unsigned __int128) st->len[i] * st->len[i]; }
+    pl->cells = (uint64_t) ((s1 * s1 - s2) / 2);
+
+    const uint32_t nclean = (uint32_t) st->clean_sorted.size();
+    const uint64_t nclean_pairs = (uint64_t) nclean * (nclean > 0 ? nclean - 1 : 0) / 2;
+
+    // Pairs with at least one dirty sequence, in the reference's orientation.
+    std::vector<uint32_t> gpairs;
+    {
+        std::vector<uint8_t> isd(n, 0);
+        bool any = false;
+        for(uint32_t i = 0; i < n; ++i) if(st->dirty[i]) { isd[i] = 1; any = true; }
+        if(any) {
+            for(uint32_t i = 1; i < n; ++i) {
+                for(uint32_t j = 0; j < i; ++j) {
+                    if(!isd[i] && !isd[j]) continue;
+                    const uint64_t bi = (st->len[i] + 2) / 3, bj = (st->len[j] + 2) / 3;
+                    gpairs.push_back(bi > bj ? i : j);
+                    gpairs.push_back(bi > bj ? j : i);
+                }
+            }
+        }
+    }
+    pl->ngeneric = gpairs.size() / 2;
+
+    uint32_t max_cols = 1;
+    for(uint32_t i = 0; i < n; ++i) max_cols = std::max(max_cols, st->plen[i]);
+    const uint64_t stride = round_up((uint64_t) max_cols + 160, 32);
+
+    // Occupancy of the per-warp kernels.
+    const size_t smem = smem_bytes<kPlainR>();
+    int bps = 0, bps3 = 0;
+    if(occupancy(nw_plain_kernel<kPlainR, kWPB>, smem, &bps) || occupancy(nw_generic_kernel<kPlainR, kWPB>, smem, &bps3))
+        return set_error(ctx, MSA_ERR_CUDA, "occupancy query failed (no sm_100a image?)");
+    bps = std::min(bps, bps3);
+    const uint64_t resident_blocks = (uint64_t) ctx->num_sms * (uint64_t) bps;
+    uint64_t warps_needed = resident_blocks * kWPB;
+
+    // Persistent task tables: rows pairs (sorted 2k, 2k+1) x column groups of W.
+    std::vector<uint64_t> row_task;
+    std::vector<uint8_t> row_narrow;
+    uint64_t ntasks = 0;
+    uint32_t K = 0;
+    if(mode == MSA_NW_PERSISTENT && nclean_pairs > 0) {
+        const int SH = 32 * tiles.R;
+        K = (nclean + 1) / 2;
+        row_task.assign(K + 1, 0);
+        row_narrow.assign(K, 0);
+        for(uint32_t k = 0; k < K; ++k) {
+            row_task[k] = ntasks;
+            const int64_t ncol = (int64_t) nclean - (2 * (int64_t) k + 1);
+            if(ncol <= 0) continue;
+            const int64_t rows_p = (int64_t) round_up(st->eff[st->clean_sorted[2 * k]], SH);
+            const int64_t cols = st->eff[st->clean_sorted[2 * k + 1]];
+            const bool nar = narrow_ok(rows_p, cols, tbl);
+            row_narrow[k] = nar ? 1 : 0;
+            const uint64_t groups = (uint64_t) (ncol + tiles.W - 1) / tiles.W;
+            if(nar) pl->narrow_tasks += (uint32_t) groups;
+            ntasks += groups;
+        }
+        row_task[K] = ntasks;
+        int rc;
+        if(tiles.R == 16 && tiles.W == 4) rc = batched_grid<16, 4>(ctx, ntasks, &pl->batch_grid);
+        else if(tiles.R == 16 && tiles.W == 8) rc = batched_grid<16, 8>(ctx, ntasks, &pl->batch_grid);
+        else if(tiles.R == 32 && tiles.W == 4) rc = batched_grid<32, 4>(ctx, ntasks, &pl->batch_grid);
+        else rc = batched_grid<32, 8>(ctx, ntasks, &pl->batch_grid);
+        if(rc) return rc;
+        warps_needed = std::max<uint64_t>(warps_needed, pl->batch_grid * tiles.W);
+    }
+
+    // One device allocation owned by the plan.
+    size_t off = 0;
+    auto take = [&off](size_t b) { size_t o = off; off = round_up(off + b, 256); return o; };
+    const size_t o_prof = take(st->prof_bytes + 64), o_ext = take(kAlpha * kAlpha),
+                 o_bound = take(warps_needed * stride * sizeof(uint32_t)), o_rt = take((K + 1) * sizeof(uint64_t)),
+                 o_rn = take(K + 16), o_gp = take(gpairs.size() * sizeof(uint32_t) + 16), o_cnt = take(64);
+    MSA_CUDA_TRY(ctx, pl->mem.ensure(off));
+    char *base = (char *) pl->mem.ptr;
+    cudaStream_t s = ctx->stream;
+    MSA_CUDA_TRY(ctx, cudaMemcpyAsync(base + o_ext, tbl.score, kAlpha * kAlpha, cudaMemcpyHostToDevice, s));
+    if(K) {
+        MSA_CUDA_TRY(ctx, cudaMemcpyAsync(base + o_rt, row_task.data(), (K + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
+        MSA_CUDA_TRY(ctx, cudaMemcpyAsync(base + o_rn, row_narrow.data(), K, cudaMemcpyHostToDevice, s));
+    }
+    if(!gpairs.empty())
+        MSA_CUDA_TRY(ctx, cudaMemcpyAsync(base + o_gp, gpairs.data(), gpairs.size() * sizeof(uint32_t),
+                                          cudaMemcpyHostToDevice, s));
+    MSA_CUDA_TRY(ctx, cudaStreamSynchronize(s));   // host vectors go out of scope
+
+    pl->d_ext = (const int8_t *) (base + o_ext);
+    NwParams &p = pl->p;
+    p.units = st->d_units;
+    p.uoff = st->d_off;
+    p.eff = st->d_eff;
+    p.plen = st->d_plen;
+    p.prof = (const int8_t *) (base + o_prof);
+    p.poff = st->d_prof_off;
+    p.plp = st->d_prof_lp;
+    p.sorted = st->d_clean_sorted;
+    p.nclean = nclean;
+    p.out = d_out;
+    p.g = tbl.penalty;
+    p.bound_stride = stride;
+    p.bound = (uint32_t *) (base + o_bound);
+    p.gpairs = (const uint32_t *) (base + o_gp);
+    p.ngeneric = pl->ngeneric;
+    pl->gen_blocks = std::min<uint64_t>(resident_blocks, (pl->ngeneric + kWPB - 1) / kWPB);
+
+    BatchParams &bp = pl->bp;
+    bp.units = st->d_units;
+    bp.uoff = st->d_off;
+    bp.eff = st->d_eff;
+    bp.prof = p.prof;
+    bp.poff = st->d_prof_off;
+    bp.plp = st->d_prof_lp;
+    bp.sorted = st->d_clean_sorted;
+    bp.nclean = nclean;
+    bp.npairs_rows = K;
+    bp.row_task = (const uint64_t *) (base + o_rt);
+    bp.row_narrow = (const uint8_t *) (base + o_rn);
+    bp.ntasks = ntasks;
+    bp.bound = p.bound;
+    bp.bound_stride = stride;
+    bp.out = d_out;
+    bp.g = tbl.penalty;
+    bp.counter = (unsigned long long *) (base + o_cnt);
+
+    pl->launches = 1 + (pl->ngeneric ? 1 : 0);
+    if(mode == MSA_NW_PLAIN && nclean_pairs > 0) {
+        // Buckets: runs of sorted rows with the same strip count.
+        constexpr int SH = 32 * kPlainR;
+        uint32_t a = 0;
+        while(a + 1 < nclean) {
+            const uint32_t strips = (st->eff[st->clean_sorted[a]] + SH - 1) / SH;
+            uint32_t a2 = a + 1;
+            while(a2 + 1 < nclean && (st->eff[st->clean_sorted[a2]] + SH - 1) / SH == strips) ++a2;
+            const uint64_t k_lo = (uint64_t) a * (2 * (uint64_t) nclean - a - 1) / 2;
+            const uint64_t k_hi = (uint64_t) a2 * (2 * (uint64_t) nclean - a2 - 1) / 2;
+            pl->plain.push_back({k_lo, k_hi, std::min<uint64_t>(resident_blocks, (k_hi - k_lo + kWPB - 1) / kWPB)});
+            a = a2;
+        }
+        pl->launches += (uint32_t) pl->plain.size();
+    } else if(ntasks > 0) {
+        pl->launches += 1;
+    }
+    return MSA_OK;
+}
+
+// Enqueues one scoring pass. Events are recorded with cudaEventRecordExternal
+// while capturing so they stay real timing records inside the graph.
+static cudaError_t enqueue(msa_ctx *ctx, const NwPlan &pl, const SeqStore *st, cudaStream_t s, bool capturing)
+{
+    const unsigned flags = capturing ? cudaEventRecordExternal : cudaEventRecordDefault;
+    cudaError_t e = cudaEventRecordWithFlags(ctx->ev[0], s, flags);
+    if(e) return e;
+    build_profiles_kernel<<<pl.n, 256, 0, s>>>(st->d_units, st->d_off, st->d_eff, st->d_prof_off, st->d_prof_lp,
+                                               pl.d_ext, const_cast<int8_t *>(pl.p.prof));
+    if((e = cudaGetLastError())) return e;
+    if((e = cudaEventRecordWithFlags(ctx->ev[1], s, flags))) return e;
+    const size_t smem = smem_bytes<kPlainR>();
+    if(pl.ngeneric) {
+        nw_generic_kernel<kPlainR, kWPB><<<(unsigned) pl.gen_blocks, kWPB * 32, smem, s>>>(pl.p);
+        if((e = cudaGetLastError())) return e;
+    }
+    if(pl.mode == MSA_NW_PLAIN) {
+        for(const PlainLaunch &L : pl.plain) {
+            nw_plain_kernel<kPlainR, kWPB><<<(unsigned) L.blocks, kWPB * 32, smem, s>>>(pl.p, L.k_lo, L.k_hi);
+            if((e = cudaGetLastError())) return e;
+        }
+    } else if(pl.bp.ntasks) {
+        if((e = cudaMemsetAsync(pl.bp.counter, 0, 64, s))) return e;
+        const Tiles t = pl.tiles;
+        if(t.R == 16 && t.W == 4) launch_batched<16, 4>(pl, s);
+        else if(t.R == 16 && t.W == 8) launch_batched<16, 8>(pl, s);
+        else if(t.R == 32 && t.W == 4) launch_batched<32, 4>(pl, s);
+        else launch_batched<32, 8>(pl, s);
+        if((e = cudaGetLastError())) return e;
+    }
+    return cudaEventRecordWithFlags(ctx->ev[2], s, flags);
+}
+
+static bool same_table(const ExtTable &a, const ExtTable &b)
+{
+    return std::memcmp(a.score, b.score, sizeof(a.score)) == 0 && std::memcmp(a.valid, b.valid, sizeof(a.valid)) == 0 &&
+           a.penalty == b.penalty;
 }
 
 int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d_out)
@@ -782,176 +1042,70 @@ int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d
     stats.pairs = (uint64_t) n * (n > 0 ? n - 1 : 0) / 2;
     if(n < 2) { ctx->last = stats; return MSA_OK; }
 
-    MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[0], s));
-
-    // 1. Score profiles for every sequence.
-    MSA_CUDA_TRY(ctx, ctx->prof.ensure(st->prof_bytes + kAlpha * kAlpha + 64));
-    int8_t *d_prof = (int8_t *) ctx->prof.ptr;
-    int8_t *d_ext = d_prof + st->prof_bytes;
-    MSA_CUDA_TRY(ctx, cudaMemcpyAsync(d_ext, tbl.score, kAlpha * kAlpha, cudaMemcpyHostToDevice, s));
-    build_profiles_kernel<<<n, 256, 0, s>>>(st->d_units, st->d_off, st->d_eff, st->d_prof_off,
-                                            st->d_prof_lp, d_ext, d_prof);
-    MSA_CUDA_TRY(ctx, cudaGetLastError());
-    ctx->launches++;
-    stats.launches++;
-
-    // 2. Plan.
     const uint32_t nclean = (uint32_t) st->clean_sorted.size();
-    const uint64_t nclean_pairs = (uint64_t) nclean * (nclean > 0 ? nclean - 1 : 0) / 2;
-    std::vector<uint32_t> gpairs;
-    {
-        // Pairs with at least one dirty sequence, in the reference's orientation.
-        std::vector<uint32_t> dirty;
-        for(uint32_t i = 0; i < n; ++i) if(st->dirty[i]) dirty.push_back(i);
-        if(!dirty.empty()) {
-            std::vector<uint8_t> isd(n, 0);
-            for(uint32_t d : dirty) isd[d] = 1;
-            for(uint32_t i = 1; i < n; ++i) {
-                for(uint32_t j = 0; j < i; ++j) {
-                    if(!isd[i] && !isd[j]) continue;
-                    const uint64_t bi = (st->len[i] + 2) / 3, bj = (st->len[j] + 2) / 3;
-                    const uint32_t r = bi > bj ? i : j, c = bi > bj ? j : i;
-                    gpairs.push_back(r);
-                    gpairs.push_back(c);
-                }
-            }
+    const Tiles tiles = mode != MSA_NW_PERSISTENT ? Tiles{0, 0}
+                      : ctx->tile_r ? Tiles{ctx->tile_r, ctx->tile_w} : pick_tiles(st, nclean);
+
+    if(!ctx->graphs) ctx->graphs = new GraphCache;
+    auto &plans = ctx->graphs->plans;
+    NwPlan *pl = nullptr;
+    for(size_t i = 0; i < plans.size(); ++i) {
+        NwPlan *c = plans[i];
+        if(c->store_serial == st->serial && c->mode == mode && c->d_out == d_out && c->tiles.R == tiles.R &&
+           c->tiles.W == tiles.W && same_table(c->tbl, tbl)) {
+            pl = c;
+            plans.erase(plans.begin() + i);
+            plans.push_back(pl);
+            break;
         }
     }
-    const uint64_t ngeneric = gpairs.size() / 2;
-
-    uint32_t max_cols = 1;
-    for(uint32_t i = 0; i < n; ++i) max_cols = std::max(max_cols, st->plen[i]);
-
-    NwParams p{};
-    p.units = st->d_units;
-    p.uoff = st->d_off;
-    p.eff = st->d_eff;
-    p.plen = st->d_plen;
-    p.prof = d_prof;
-    p.poff = st->d_prof_off;
-    p.plp = st->d_prof_lp;
-    p.sorted = st->d_clean_sorted;
-    p.nclean = nclean;
-    p.out = d_out;
-    p.g = tbl.penalty;
-    p.bound_stride = round_up((uint64_t) max_cols + 160, 32);
-
-    auto kplain = nw_plain_kernel<kPlainR, kWPB>;
-    auto kgen = nw_generic_kernel<kPlainR, kWPB>;
-    const size_t smem = smem_bytes<kPlainR>();
-    int bps = 0;
-    if(occupancy(kplain, smem, &bps)) return set_error(ctx, MSA_ERR_CUDA, "occupancy query failed (no sm_100a image?)");
-    int bps3 = 0;
-    if(occupancy(kgen, smem, &bps3)) return set_error(ctx, MSA_ERR_CUDA, "occupancy query failed");
-    bps = std::min(bps, bps3);
-    const uint64_t resident_blocks = (uint64_t) ctx->num_sms * (uint64_t) bps;
-    const uint64_t resident_warps = resident_blocks * kWPB;
-
-    MSA_CUDA_TRY(ctx, ctx->bound.ensure(resident_warps * p.bound_stride * sizeof(uint32_t)));
-    p.bound = (uint32_t *) ctx->bound.ptr;
-
-    MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[1], s));
-
-    if(ngeneric > 0) {
-        MSA_CUDA_TRY(ctx, ctx->pairs.ensure(gpairs.size() * sizeof(uint32_t)));
-        MSA_CUDA_TRY(ctx, cudaMemcpyAsync(ctx->pairs.ptr, gpairs.data(), gpairs.size() * sizeof(uint32_t),
-                                          cudaMemcpyHostToDevice, s));
-        p.gpairs = (const uint32_t *) ctx->pairs.ptr;
-        p.ngeneric = ngeneric;
-        const uint64_t blocks = std::min<uint64_t>(resident_blocks, (ngeneric + kWPB - 1) / kWPB);
-        kgen<<<(unsigned) blocks, kWPB * 32, smem, s>>>(p);
-        MSA_CUDA_TRY(ctx, cudaGetLastError());
-        ctx->launches++;
-        stats.launches++;
+    if(!pl) {
+        while(plans.size() >= kMaxPlans) { delete plans.front(); plans.erase(plans.begin()); }
+        pl = new NwPlan;
+        const int rc = build_plan(ctx, st, tbl, mode, d_out, tiles, pl);
+        if(rc) { delete pl; return rc; }
+        plans.push_back(pl);
     }
 
-    if(nclean_pairs > 0) {
-        if(mode == MSA_NW_PLAIN) {
-            // Buckets: runs of sorted rows with the same strip count.
-            constexpr int SH = 32 * kPlainR;
-            uint32_t a = 0;
-            while(a + 1 < nclean) {
-                const uint32_t strips = (st->eff[st->clean_sorted[a]] + SH - 1) / SH;
-                uint32_t a2 = a + 1;
-                while(a2 + 1 < nclean && (st->eff[st->clean_sorted[a2]] + SH - 1) / SH == strips) ++a2;
-                const uint64_t k_lo = (uint64_t) a * (2 * (uint64_t) nclean - a - 1) / 2;
-                const uint64_t k_hi = (uint64_t) a2 * (2 * (uint64_t) nclean - a2 - 1) / 2;
-                const uint64_t warps = k_hi - k_lo;
-                const uint64_t blocks = std::min<uint64_t>(resident_blocks, (warps + kWPB - 1) / kWPB);
-                kplain<<<(unsigned) blocks, kWPB * 32, smem, s>>>(p, k_lo, k_hi);
-                MSA_CUDA_TRY(ctx, cudaGetLastError());
-                ctx->launches++;
-                stats.launches++;
-                a = a2;
-            }
+    // The persistent mode replays a captured graph; the legacy default stream
+    // cannot be captured, so there the same sequence is launched directly.
+    bool use_graph = mode == MSA_NW_PERSISTENT && s != nullptr;
+    if(use_graph && (!pl->exec || pl->captured_on != s)) {
+        if(pl->exec) { cudaGraphExecDestroy(pl->exec); pl->exec = nullptr; }
+        cudaGraph_t g = nullptr;
+        cudaError_t e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if(!e) {
+            const cudaError_t e2 = enqueue(ctx, *pl, st, s, true);
+            e = cudaStreamEndCapture(s, &g);
+            if(!e) e = e2;
+        }
+        if(!e) e = cudaGraphInstantiate(&pl->exec, g, 0);
+        if(g) cudaGraphDestroy(g);
+        if(e) {
+            cudaGetLastError();
+            pl->exec = nullptr;
+            use_graph = false;   // launch the same kernels directly
         } else {
-            // Rows pairs (sorted 2k, 2k+1) against column groups of W sequences.
-            const Tiles tl = ctx->tile_r ? Tiles{ctx->tile_r, ctx->tile_w} : pick_tiles(st, nclean);
-            const int SH = 32 * tl.R;
-            const uint32_t K = (nclean + 1) / 2;
-            std::vector<uint64_t> row_task(K + 1, 0);
-            std::vector<uint8_t> row_narrow(K, 0);
-            uint64_t q = 0;
-            uint32_t narrow_tasks = 0;
-            for(uint32_t k = 0; k < K; ++k) {
-                row_task[k] = q;
-                const int64_t ncol = (int64_t) nclean - (2 * (int64_t) k + 1);
-                if(ncol <= 0) continue;
-                const int64_t rows_p = (int64_t) round_up(st->eff[st->clean_sorted[2 * k]], SH);
-                const int64_t cols = st->eff[st->clean_sorted[2 * k + 1]];
-                const bool nar = narrow_ok(rows_p, cols, tbl);
-                row_narrow[k] = nar ? 1 : 0;
-                const uint64_t groups = (uint64_t) (ncol + tl.W - 1) / tl.W;
-                if(nar) narrow_tasks += (uint32_t) groups;
-                q += groups;
-            }
-            row_task[K] = q;
-            stats.narrow_tasks = narrow_tasks;
-            const size_t tb = (K + 1) * sizeof(uint64_t) + K + 16;
-            MSA_CUDA_TRY(ctx, ctx->tasks.ensure(tb));
-            MSA_CUDA_TRY(ctx, ctx->counters.ensure(64));
-            uint64_t *d_rt = (uint64_t *) ctx->tasks.ptr;
-            uint8_t *d_rn = (uint8_t *) (d_rt + K + 1);
-            MSA_CUDA_TRY(ctx, cudaMemcpyAsync(d_rt, row_task.data(), (K + 1) * sizeof(uint64_t), cudaMemcpyHostToDevice, s));
-            MSA_CUDA_TRY(ctx, cudaMemcpyAsync(d_rn, row_narrow.data(), K, cudaMemcpyHostToDevice, s));
-            MSA_CUDA_TRY(ctx, cudaMemsetAsync(ctx->counters.ptr, 0, 64, s));
-            BatchParams bp{};
-            bp.units = st->d_units;
-            bp.uoff = st->d_off;
-            bp.eff = st->d_eff;
-            bp.prof = d_prof;
-            bp.poff = st->d_prof_off;
-            bp.plp = st->d_prof_lp;
-            bp.sorted = st->d_clean_sorted;
-            bp.nclean = nclean;
-            bp.npairs_rows = K;
-            bp.row_task = d_rt;
-            bp.row_narrow = d_rn;
-            bp.ntasks = q;
-            bp.bound_stride = p.bound_stride;
-            bp.out = d_out;
-            bp.g = tbl.penalty;
-            bp.counter = (unsigned long long *) ctx->counters.ptr;
-            int rc = MSA_OK;
-            if(tl.R == 16 && tl.W == 4) rc = launch_batched<16, 4>(ctx, bp, q, &stats.launches);
-            else if(tl.R == 16 && tl.W == 8) rc = launch_batched<16, 8>(ctx, bp, q, &stats.launches);
-            else if(tl.R == 32 && tl.W == 4) rc = launch_batched<32, 4>(ctx, bp, q, &stats.launches);
-            else rc = launch_batched<32, 8>(ctx, bp, q, &stats.launches);
-            if(rc) return rc;
+            pl->captured_on = s;
         }
     }
+    if(use_graph) {
+        MSA_CUDA_TRY(ctx, cudaGraphLaunch(pl->exec, s));
+    } else {
+        MSA_CUDA_TRY(ctx, enqueue(ctx, *pl, st, s, false));
+    }
+    ctx->launches += pl->launches;
 
-    MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[2], s));
     MSA_CUDA_TRY(ctx, cudaEventSynchronize(ctx->ev[2]));
     float ms_k = 0, ms_t = 0;
     cudaEventElapsedTime(&ms_k, ctx->ev[1], ctx->ev[2]);
     cudaEventElapsedTime(&ms_t, ctx->ev[0], ctx->ev[2]);
     stats.kernel_ms = ms_k;
     stats.total_ms = ms_t;
-    // sum over pairs of L_i * L_j = ((sum L)^2 - sum L^2) / 2, in 128-bit arithmetic.
-    unsigned __int128 s1 = 0, s2 = 0;
-    for(uint32_t i = 0; i < n; ++i) { s1 += st->len[i]; s2 += (unsigned __int128) st->len[i] * st->len[i]; }
-    stats.cells = (uint64_t) ((s1 * s1 - s2) / 2);
+    stats.cells = pl->cells;
+    stats.launches = pl->launches;
+    stats.narrow_tasks = pl->narrow_tasks;
+    stats.graph = use_graph ? 1 : 0;
     ctx->last = stats;
     return MSA_OK;
 }

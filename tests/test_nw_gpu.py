@@ -165,3 +165,25 @@ def test_wide_rows_pairs_match_oracle(gpu, tables):
     got = gpu_scores(wl, "blosum62", _lib.MSA_NW_PERSISTENT)
     assert np.array_equal(got, oracle_scores(wl, "blosum62", tables))
     assert pairwise.last_stats().narrow_tasks == 0
+
+
+def test_repeated_call_replays_graph_with_identical_scores(gpu, tables):
+    wl = W.random_set(50, 40, 50, 900)
+    flat, offs, lens = wl.flat_units()
+    lib = _lib.lib()
+    h = ctypes.c_uint64()
+    u8, u64 = ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint64)
+    _lib.check(lib.msa_seqs_upload(gpu.handle, flat.ctypes.data_as(u8), offs.ctypes.data_as(u64),
+                                   lens.ctypes.data_as(u64), wl.n, ctypes.byref(h)), gpu.handle)
+    t = ScoringTable("blosum62")
+    outs, graphs = [], []
+    for _ in range(3):
+        out = np.zeros(wl.n * (wl.n - 1) // 2, np.int32)
+        _lib.check(lib.msa_nw_all_pairs(gpu.handle, h.value, ctypes.byref(t._t), _lib.MSA_NW_PERSISTENT,
+                                        out.ctypes.data_as(ctypes.c_void_p), 0), gpu.handle)
+        outs.append(out)
+        graphs.append(pairwise.last_stats().graph)
+    lib.msa_seqs_release(gpu.handle, h.value)
+    assert graphs == [1, 1, 1]
+    want = oracle_scores(wl, "blosum62", tables)
+    assert all(np.array_equal(o, want) for o in outs)
