@@ -183,6 +183,87 @@ def probe_ops(iters: int = 2048) -> dict:
     return res
 
 
+def serve_bench(args):
+    """c5: all-pairs jobs (n U[8,512], lengths U[50,2000], half protein/blosum62,
+    half DNA/default) arriving as a Poisson process at `load` x the saturated
+    rate; latency = completion - submission per job. Compared with the same
+    arrivals served one at a time by the plain kernel."""
+    import ctypes
+    import threading
+
+    from msa_b200 import ScoringTable, _lib, pairwise
+    from msa_b200 import workloads as W
+    from msa_b200.serve import Server
+    jobs = [W.c5_job(50_000 + k) for k in range(args.jobs)]
+    packed = [(wl.flat_units(), ScoringTable(wl.table), wl.cells()) for wl in jobs]
+    total_cells = sum(c for _, _, c in packed)
+    mean_cells = total_cells / len(jobs)
+
+    # Saturated throughput: every job submitted at once.
+    with Server(device=0) as srv:
+        t0 = time.perf_counter()
+        ids = [srv.submit(*fu, t) for fu, t, _ in packed]
+        for i in ids:
+            srv.wait(i)
+        sat_s = time.perf_counter() - t0
+    sat_gcups = total_cells / sat_s / 1e9
+
+    rate = args.load * (sat_gcups * 1e9) / mean_cells          # jobs per second
+    rng = np.random.Generator(np.random.PCG64(5))
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(jobs)))
+
+    def run_server():
+        stats = [None] * len(jobs)
+        with Server(device=0) as srv:
+            ids = [None] * len(jobs)
+            start = time.perf_counter()
+
+            def producer():
+                for k, (fu, t, _) in enumerate(packed):
+                    delay = arrivals[k] - (time.perf_counter() - start)
+                    if delay > 0:
+                        time.sleep(delay)
+                    ids[k] = srv.submit(*fu, t)
+            th = threading.Thread(target=producer)
+            th.start()
+            for k in range(len(jobs)):
+                while ids[k] is None:
+                    time.sleep(0.0005)
+                stats[k] = srv.wait(ids[k])[1]
+            th.join()
+        lat = np.array([s["latency_ms"] for s in stats])
+        span_ms = max(s["done_ms"] for s in stats) - min(s["submit_ms"] for s in stats)
+        return lat, total_cells / (span_ms / 1e3) / 1e9, stats
+
+    lat, agg, stats = run_server()
+
+    # Same jobs, same arrivals, one at a time through the plain kernel.
+    def run_plain():
+        start = time.perf_counter()
+        lat_p = []
+        for k, (fu, t, _) in enumerate(packed):
+            now = time.perf_counter() - start
+            if now < arrivals[k]:
+                time.sleep(arrivals[k] - now)
+            pairwise.score_units(*fu, t, _lib.MSA_NW_PLAIN)
+            lat_p.append((time.perf_counter() - start - arrivals[k]) * 1e3)
+        span = time.perf_counter() - start - arrivals[0]
+        return np.array(lat_p), total_cells / span / 1e9
+
+    lat_p, agg_p = run_plain()
+    line = {"metric": "serve p50/p99 job latency (continuous batching)", "unit": "ms",
+            "p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+            "p99_over_p50": float(np.percentile(lat, 99) / np.percentile(lat, 50)),
+            "aggregate_gcups": agg, "saturated_gcups": sat_gcups, "offered_load": args.load,
+            "arrival_rate_per_s": rate, "jobs": len(jobs), "mean_cells_per_job": mean_cells,
+            "mean_launches_per_job": float(np.mean([s["launches"] for s in stats])),
+            "plain_one_at_a_time": {"p50_ms": float(np.percentile(lat_p, 50)),
+                                    "p99_ms": float(np.percentile(lat_p, 99)), "aggregate_gcups": agg_p},
+            "data": "synthetic (seeded c5 jobs)"}
+    print(json.dumps(line))
+    return line
+
+
 def profile_run(args):
     """One scoring call (after warm-up) for ncu captures; prints its stats."""
     import ctypes
@@ -230,9 +311,14 @@ def main():
                     help="profiling run: --warmup calls then one call, on the first --n sequences")
     ap.add_argument("--n", type=int, default=0, help="with --profile: use the first N sequences")
     ap.add_argument("--probe", action="store_true", help="integer-op throughput probes (lane-ops/clk/SM)")
+    ap.add_argument("--serve", action="store_true", help="serving loop: Poisson arrivals of c5 jobs")
+    ap.add_argument("--jobs", type=int, default=160)
+    ap.add_argument("--load", type=float, default=0.8, help="offered load as a fraction of saturated throughput")
     args = ap.parse_args()
     if args.probe:
         return probe_ops()
+    if args.serve:
+        return serve_bench(args)
     if args.impl == "reference":
         return reference_arm(args)
     if args.profile:

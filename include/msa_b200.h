@@ -230,6 +230,43 @@ typedef struct msa_nj_stats {
 } msa_nj_stats;
 int msa_nj_last_stats(const msa_ctx *ctx, msa_nj_stats *out);
 
+/* ---------------------------------------------------------------- serving */
+
+typedef struct msa_server msa_server;
+
+typedef struct msa_serve_config {
+    int device;
+    uint64_t hbm_budget_bytes;  /* 0 = 80 % of free device memory at start */
+    uint32_t max_jobs;          /* admitted jobs at once; 0 = 64 */
+    uint32_t quantum_pairs;     /* pairs per merged launch quantum; 0 = auto */
+} msa_serve_config;
+
+typedef struct msa_job_stats {
+    double submit_ms;   /* host monotonic clock, ms */
+    double admit_ms;
+    double done_ms;
+    uint64_t cells;
+    uint32_t n;
+    uint32_t launches;  /* merged launches this job's tiles were part of */
+} msa_job_stats;
+
+/* Starts a serving loop (continuous batching of all-pairs jobs) on a thread
+ * owning its own context. No counterpart in the reference, which scores one
+ * database per process run (src/museqa.cpp:223-236). Jobs are admitted in
+ * arrival order while their device footprint fits the HBM budget; every
+ * merged launch takes tasks round-robin from all admitted jobs. */
+int msa_serve_start(const msa_serve_config *cfg, msa_server **out);
+/* Queues an all-pairs job (same inputs as msa_seqs_upload + table). */
+int msa_serve_submit(msa_server *srv, const uint8_t *units, const uint64_t *offs,
+                     const uint64_t *lens, uint32_t n, const msa_table *table,
+                     uint64_t *job_id);
+/* Waits up to timeout_ms (-1 = forever) for a job; copies n(n-1)/2 scores
+ * (index i(i-1)/2+j, as msa_nw_all_pairs) into `out` and releases the job.
+ * MSA_ERR_DEVICE_TIMEOUT if it is not done yet (the job stays queued). */
+int msa_serve_wait(msa_server *srv, uint64_t job_id, int timeout_ms, int32_t *out,
+                   msa_job_stats *stats);
+int msa_serve_stop(msa_server *srv);
+
 /* ------------------------------------------------------------ diagnostics */
 
 /*

@@ -17,7 +17,7 @@ LIB = PKG / "libmsa_b200.so"
 BUILD_DIR = PKG / "_build"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["tables.cpp", "abi.cpp", "nw_kernels.cu", "nj_kernel.cu", "probe.cu", "noalloc.cu"]
+SOURCES = ["tables.cpp", "abi.cpp", "nw_kernels.cu", "nj_kernel.cu", "probe.cu", "noalloc.cu", "serve.cpp"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", "-I", str(INCLUDE)]
 

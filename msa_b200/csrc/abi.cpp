@@ -127,8 +127,14 @@ void *msa_get_stream(msa_ctx *ctx) { return ctx ? (void *) ctx->stream : nullptr
 
 uint64_t msa_launch_count(const msa_ctx *ctx) { return ctx ? ctx->launches : 0; }
 
-int msa_seqs_upload(msa_ctx *ctx, const uint8_t *units, const uint64_t *offs, const uint64_t *lens,
-                    uint32_t n, msa_seqs *out)
+}  // extern "C"
+
+namespace msa {
+
+// Builds a device-resident store (the work of msa_seqs_upload without the
+// handle). On failure nothing is left allocated.
+int build_store(msa_ctx *ctx, const uint8_t *units, const uint64_t *offs, const uint64_t *lens, uint32_t n,
+                SeqStore **out)
 {
     if(!ctx || !out || (n && (!offs || !lens))) return MSA_ERR_INVALID;
     SeqStore *st = nullptr;
@@ -214,18 +220,40 @@ int msa_seqs_upload(msa_ctx *ctx, const uint8_t *units, const uint64_t *offs, co
         if(e) { free_store(st); return cuda_error(ctx, e, "sequence upload"); }
         static std::atomic<uint64_t> serials{1};
         st->serial = serials++;
-        const uint64_t h = ctx->next_handle++;
-        ctx->stores[h] = st;
-        *out = h;
+        *out = st;
         return MSA_OK;
     } catch(const std::bad_alloc &) {
         free_store(st);
         return set_error(ctx, MSA_ERR_NOMEM, "host allocation failed");
     } catch(...) {
         free_store(st);
-        return set_error(ctx, MSA_ERR_CUDA, "unexpected failure in msa_seqs_upload");
+        return set_error(ctx, MSA_ERR_CUDA, "unexpected failure building a sequence store");
     }
 }
+
+void destroy_store(SeqStore *st) { free_store(st); }
+
+}  // namespace msa
+
+extern "C" int msa_seqs_upload(msa_ctx *ctx, const uint8_t *units, const uint64_t *offs, const uint64_t *lens,
+                               uint32_t n, msa_seqs *out)
+{
+    if(!ctx || !out) return MSA_ERR_INVALID;
+    SeqStore *st = nullptr;
+    const int rc = msa::build_store(ctx, units, offs, lens, n, &st);
+    if(rc) return rc;
+    try {
+        const uint64_t h = ctx->next_handle++;
+        ctx->stores[h] = st;
+        *out = h;
+        return MSA_OK;
+    } catch(...) {
+        free_store(st);
+        return set_error(ctx, MSA_ERR_NOMEM, "host allocation failed");
+    }
+}
+
+extern "C" {
 
 int msa_seqs_release(msa_ctx *ctx, msa_seqs seqs)
 {

@@ -112,6 +112,31 @@ constexpr int kUnitFront = 64;
 int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out);
 
 void release_graphs(msa_ctx *ctx);
+int build_store(msa_ctx *ctx, const uint8_t *units, const uint64_t *offs, const uint64_t *lens, uint32_t n,
+                SeqStore **out);
+void destroy_store(SeqStore *st);
+// Tile shape of the batched kernels for a store (committed autotuner table).
+struct Tiles { int R, W; };
+Tiles pick_tiles_for(const SeqStore *st);
+// Score profiles of every sequence of a store into d_prof (st->prof_bytes).
+cudaError_t launch_profiles(const SeqStore *st, const int8_t *d_ext, int8_t *d_prof, cudaStream_t s);
+// 16-bit flag and column-group count of each rows pair (sorted 2k, 2k+1).
+void plan_rows_pairs(const SeqStore *st, const ExtTable &tbl, Tiles tiles, std::vector<uint8_t> &narrow,
+                     std::vector<uint32_t> &groups);
+// One merged launch of the serving kernel (tiles 32 x 8) over `ntasks` tasks.
+struct ServeLaunch {
+    const void *jobs;        // JobView[slots], device
+    const void *tasks;       // uint4[ntasks] (slot, rows pair, group, 0), device
+    uint64_t ntasks;
+    uint32_t *bound;
+    uint64_t bound_stride;
+    unsigned long long *counter;
+};
+int serve_grid(msa_ctx *ctx, uint64_t *grid);
+cudaError_t launch_serve(const ServeLaunch &l, uint64_t grid, cudaStream_t s);
+size_t job_view_bytes();
+void fill_job_view(void *dst, const SeqStore *st, const int8_t *d_prof, const uint8_t *d_narrow, int32_t *d_out,
+                   int32_t g);
 void drop_plans_for_store(msa_ctx *ctx, uint64_t serial);
 int set_error(msa_ctx *ctx, int status, const std::string &msg);
 int cuda_error(msa_ctx *ctx, cudaError_t e, const char *what);

@@ -366,23 +366,40 @@ __global__ void __launch_bounds__(WPB * 32) nw_plain_kernel(NwParams p, uint64_t
 // CTAs take tasks from a global counter in cost order (longest rows pairs
 // first), so the tail of the launch is the cheapest work.
 
-struct BatchParams {
+// One all-pairs job as the batched kernels see it: its store, score profiles,
+// length order, per-rows-pair 16-bit flags and output triangle.
+struct JobView {
     const uint8_t *units;
     const uint64_t *uoff;
     const uint32_t *eff;
     const int8_t *prof;
     const uint64_t *poff;
     const uint32_t *plp;
-    const uint32_t *sorted;
+    const uint32_t *sorted;     // clean sequences, eff descending
+    const uint8_t *row_narrow;  // 16-bit lanes for rows pair k
+    int32_t *out;
     uint32_t nclean;
+    int32_t g;
+};
+
+struct BatchParams {
+    JobView job;
     uint32_t npairs_rows;       // number of rows pairs, ceil(nclean / 2)
     const uint64_t *row_task;   // first task of each rows pair (npairs_rows + 1)
-    const uint8_t *row_narrow;  // 16-bit tasks for this rows pair
     uint64_t ntasks;
     uint32_t *bound;
     uint64_t bound_stride;
-    int32_t *out;
-    int32_t g;
+    unsigned long long *counter;
+};
+
+// Merged launches of the serving loop: explicit (job slot, rows pair, column
+// group) tasks over several jobs.
+struct ServeParams {
+    const JobView *jobs;
+    const uint4 *tasks;
+    uint64_t ntasks;
+    uint32_t *bound;
+    uint64_t bound_stride;
     unsigned long long *counter;
 };
 
@@ -584,6 +601,59 @@ __device__ __forceinline__ void strip_plan(int rows, int &nst, int &R)
 // Resident CTAs per SM the batched kernel is compiled for (register budget).
 template <int RMAX, int W> struct BatchOcc { static constexpr int value = (RMAX == 32 ? 16 : 24) / W; };
 
+// One task: rows pair k (sorted 2k, 2k+1) of job `jv` against column group
+// `grp` (sorted 2k+1 + grp*W + warp for each warp). All threads of the CTA call it.
+template <int RMAX, int W>
+__device__ __forceinline__ void rows_pair_task(const JobView &jv, uint32_t k, uint32_t grp, uint32_t *sprof_b,
+                                               uint32_t *bound, int warp, int lane)
+{
+    const uint32_t a1 = 2 * k, a2 = min(2 * k + 1, jv.nclean - 1);
+    const uint32_t b = 2 * k + 1 + grp * W + warp;
+    const bool has = b < jv.nclean;
+    const uint32_t x1 = jv.sorted[a1], x2 = jv.sorted[a2];
+    const uint32_t y = has ? jv.sorted[b] : x1;
+    const int e1 = (int) jv.eff[x1], e2 = (int) jv.eff[x2];
+    const int ncols = has ? (int) jv.eff[y] : 0;
+    const uint8_t *cols = jv.units + jv.uoff[y];
+
+    if(jv.row_narrow[k]) {
+        // Row zero of the DP as the boundary above the first strip.
+        if(has) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = dev::dup16(-(jj + 1) * jv.g);
+        int nst, R;
+        dev::strip_plan<RMAX>(e1, nst, R);
+        int32_t r1 = 0, r2 = 0;
+        const int8_t *g1 = jv.prof + jv.poff[x1], *g2 = jv.prof + jv.poff[x2];
+        const uint32_t lp1 = jv.plp[x1], lp2 = jv.plp[x2];
+#define MSA_NARROW(RR) case RR: dev::narrow_task<RR>(sprof_b, g1, lp1, g2, lp2, e1, e2, nst, has, cols, ncols, bound, jv.g, lane, r1, r2); break;
+        switch(R) {
+            MSA_NARROW(4) MSA_NARROW(8) MSA_NARROW(12) MSA_NARROW(16)
+            default:
+                if constexpr(RMAX > 16) {
+                    switch(R) { MSA_NARROW(20) MSA_NARROW(24) MSA_NARROW(28) MSA_NARROW(32) default: break; }
+                }
+                break;
+        }
+#undef MSA_NARROW
+        if(has && lane == 0) {
+            jv.out[dev::tri_index(x1, y)] = r1;
+            if(b != a2) jv.out[dev::tri_index(x2, y)] = r2;
+        }
+    } else {
+        for(int h = 0; h < 2; ++h) {
+            if(h == 1 && a2 == a1) break;   // CTA-uniform
+            const uint32_t xr = h ? x2 : x1;
+            const int er = h ? e2 : e1;
+            const bool mine = has && !(h == 1 && b == a2);
+            if(mine) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = (uint32_t) (-(jj + 1) * jv.g);
+            int32_t res = 0;
+            const int nst = (er + 32 * RMAX - 1) / (32 * RMAX);
+            dev::wide_task<RMAX>(sprof_b, jv.prof + jv.poff[xr], jv.plp[xr], er, nst, mine, cols, ncols, bound,
+                                 jv.g, lane, res);
+            if(mine && lane == 0) jv.out[dev::tri_index(xr, y)] = res;
+        }
+    }
+}
+
 template <int RMAX, int W>
 __global__ void __launch_bounds__(W * 32, BatchOcc<RMAX, W>::value) nw_batched_kernel(BatchParams p)
 {
@@ -603,53 +673,27 @@ __global__ void __launch_bounds__(W * 32, BatchOcc<RMAX, W>::value) nw_batched_k
             const uint32_t mid = (lo + hi + 1) >> 1;
             if(p.row_task[mid] <= q) lo = mid; else hi = mid - 1;
         }
-        const uint32_t k = lo;
-        const uint32_t grp = (uint32_t) (q - p.row_task[k]);
-        const uint32_t a1 = 2 * k, a2 = min(2 * k + 1, p.nclean - 1);
-        const uint32_t b = 2 * k + 1 + grp * W + warp;
-        const bool has = b < p.nclean;
-        const uint32_t x1 = p.sorted[a1], x2 = p.sorted[a2];
-        const uint32_t y = has ? p.sorted[b] : x1;
-        const int e1 = (int) p.eff[x1], e2 = (int) p.eff[x2];
-        const int ncols = has ? (int) p.eff[y] : 0;
-        const uint8_t *cols = p.units + p.uoff[y];
+        rows_pair_task<RMAX, W>(p.job, lo, (uint32_t) (q - p.row_task[lo]), sprof_b, bound, warp, lane);
+    }
+}
 
-        if(p.row_narrow[k]) {
-            // Row zero of the DP as the boundary above the first strip.
-            if(has) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = dev::dup16(-(jj + 1) * p.g);
-            int nst, R;
-            dev::strip_plan<RMAX>(e1, nst, R);
-            int32_t r1 = 0, r2 = 0;
-            const int8_t *g1 = p.prof + p.poff[x1], *g2 = p.prof + p.poff[x2];
-            const uint32_t lp1 = p.plp[x1], lp2 = p.plp[x2];
-#define MSA_NARROW(RR) case RR: dev::narrow_task<RR>(sprof_b, g1, lp1, g2, lp2, e1, e2, nst, has, cols, ncols, bound, p.g, lane, r1, r2); break;
-            switch(R) {
-                MSA_NARROW(4) MSA_NARROW(8) MSA_NARROW(12) MSA_NARROW(16)
-                default:
-                    if constexpr(RMAX > 16) {
-                        switch(R) { MSA_NARROW(20) MSA_NARROW(24) MSA_NARROW(28) MSA_NARROW(32) default: break; }
-                    }
-                    break;
-            }
-#undef MSA_NARROW
-            if(has && lane == 0) {
-                p.out[dev::tri_index(x1, y)] = r1;
-                if(b != a2) p.out[dev::tri_index(x2, y)] = r2;
-            }
-        } else {
-            for(int h = 0; h < 2; ++h) {
-                if(h == 1 && a2 == a1) break;   // CTA-uniform
-                const uint32_t xr = h ? x2 : x1;
-                const int er = h ? e2 : e1;
-                const bool mine = has && !(h == 1 && b == a2);
-                if(mine) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = (uint32_t) (-(jj + 1) * p.g);
-                int32_t res = 0;
-                const int nst = (er + 32 * RMAX - 1) / (32 * RMAX);
-                dev::wide_task<RMAX>(sprof_b, p.prof + p.poff[xr], p.plp[xr], er, nst, mine, cols, ncols, bound,
-                                     p.g, lane, res);
-                if(mine && lane == 0) p.out[dev::tri_index(xr, y)] = res;
-            }
-        }
+template <int RMAX, int W>
+__global__ void __launch_bounds__(W * 32, BatchOcc<RMAX, W>::value) nw_serve_kernel(ServeParams p)
+{
+    extern __shared__ __align__(16) uint32_t sprof_b[];
+    __shared__ unsigned long long task_q;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t *bound = p.bound + ((uint64_t) blockIdx.x * W + warp) * p.bound_stride;
+
+    for(;;) {
+        __syncthreads();
+        if(threadIdx.x == 0) task_q = atomicAdd(p.counter, 1ull);
+        __syncthreads();
+        const unsigned long long q = task_q;
+        if(q >= p.ntasks) break;
+        const uint4 t = p.tasks[q];
+        const JobView jv = p.jobs[t.x];
+        rows_pair_task<RMAX, W>(jv, t.y, t.z, sprof_b, bound, warp, lane);
     }
 }
 
@@ -751,8 +795,81 @@ static inline bool narrow_ok(int64_t rows_p, int64_t cols, const ExtTable &t)
 }
 
 // Batched-kernel tile shapes: rows per lane R and warps per CTA W.
-struct Tiles { int R, W; };
 #include "autotune.inc"
+
+Tiles pick_tiles_for(const SeqStore *st) { return pick_tiles(st, (uint32_t) st->clean_sorted.size()); }
+
+cudaError_t launch_profiles(const SeqStore *st, const int8_t *d_ext, int8_t *d_prof, cudaStream_t s)
+{
+    if(st->n == 0) return cudaSuccess;
+    build_profiles_kernel<<<st->n, 256, 0, s>>>(st->d_units, st->d_off, st->d_eff, st->d_prof_off, st->d_prof_lp,
+                                                d_ext, d_prof);
+    return cudaGetLastError();
+}
+
+void plan_rows_pairs(const SeqStore *st, const ExtTable &tbl, Tiles tiles, std::vector<uint8_t> &narrow,
+                     std::vector<uint32_t> &groups)
+{
+    const uint32_t nclean = (uint32_t) st->clean_sorted.size();
+    const uint32_t K = (nclean + 1) / 2;
+    const int SH = 32 * tiles.R;
+    narrow.assign(K, 0);
+    groups.assign(K, 0);
+    for(uint32_t k = 0; k < K; ++k) {
+        const int64_t ncol = (int64_t) nclean - (2 * (int64_t) k + 1);
+        if(ncol <= 0) continue;
+        const int64_t rows_p = (int64_t) round_up(st->eff[st->clean_sorted[2 * k]], SH);
+        const int64_t cols = st->eff[st->clean_sorted[2 * k + 1]];
+        narrow[k] = narrow_ok(rows_p, cols, tbl) ? 1 : 0;
+        groups[k] = (uint32_t) ((ncol + tiles.W - 1) / tiles.W);
+    }
+}
+
+size_t job_view_bytes() { return sizeof(JobView); }
+
+void fill_job_view(void *dst, const SeqStore *st, const int8_t *d_prof, const uint8_t *d_narrow, int32_t *d_out,
+                   int32_t g)
+{
+    JobView v{};
+    v.units = st->d_units;
+    v.uoff = st->d_off;
+    v.eff = st->d_eff;
+    v.prof = d_prof;
+    v.poff = st->d_prof_off;
+    v.plp = st->d_prof_lp;
+    v.sorted = st->d_clean_sorted;
+    v.row_narrow = d_narrow;
+    v.out = d_out;
+    v.nclean = (uint32_t) st->clean_sorted.size();
+    v.g = g;
+    std::memcpy(dst, &v, sizeof(v));
+}
+
+int serve_grid(msa_ctx *ctx, uint64_t *grid)
+{
+    auto kern = nw_serve_kernel<32, 8>;
+    const size_t smem = (size_t) kAlpha * 32 * 32 * 4;
+    MSA_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    int bps = 0;
+    MSA_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&bps, kern, 8 * 32, smem));
+    if(bps < 1) return set_error(ctx, MSA_ERR_CUDA, "serving kernel cannot be resident");
+    *grid = (uint64_t) ctx->num_sms * bps;
+    return MSA_OK;
+}
+
+cudaError_t launch_serve(const ServeLaunch &l, uint64_t grid, cudaStream_t s)
+{
+    ServeParams p{};
+    p.jobs = (const JobView *) l.jobs;
+    p.tasks = (const uint4 *) l.tasks;
+    p.ntasks = l.ntasks;
+    p.bound = l.bound;
+    p.bound_stride = l.bound_stride;
+    p.counter = l.counter;
+    const size_t smem = (size_t) kAlpha * 32 * 32 * 4;
+    nw_serve_kernel<32, 8><<<(unsigned) std::min<uint64_t>(grid, std::max<uint64_t>(l.ntasks, 1)), 8 * 32, smem, s>>>(p);
+    return cudaGetLastError();
+}
 
 
 // ---------------------------------------------------------------- plans and graphs
@@ -956,22 +1073,22 @@ static int build_plan(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode,
     pl->gen_blocks = std::min<uint64_t>(resident_blocks, (pl->ngeneric + kWPB - 1) / kWPB);
 
     BatchParams &bp = pl->bp;
-    bp.units = st->d_units;
-    bp.uoff = st->d_off;
-    bp.eff = st->d_eff;
-    bp.prof = p.prof;
-    bp.poff = st->d_prof_off;
-    bp.plp = st->d_prof_lp;
-    bp.sorted = st->d_clean_sorted;
-    bp.nclean = nclean;
+    bp.job.units = st->d_units;
+    bp.job.uoff = st->d_off;
+    bp.job.eff = st->d_eff;
+    bp.job.prof = p.prof;
+    bp.job.poff = st->d_prof_off;
+    bp.job.plp = st->d_prof_lp;
+    bp.job.sorted = st->d_clean_sorted;
+    bp.job.nclean = nclean;
+    bp.job.row_narrow = (const uint8_t *) (base + o_rn);
+    bp.job.out = d_out;
+    bp.job.g = tbl.penalty;
     bp.npairs_rows = K;
     bp.row_task = (const uint64_t *) (base + o_rt);
-    bp.row_narrow = (const uint8_t *) (base + o_rn);
     bp.ntasks = ntasks;
     bp.bound = p.bound;
     bp.bound_stride = stride;
-    bp.out = d_out;
-    bp.g = tbl.penalty;
     bp.counter = (unsigned long long *) (base + o_cnt);
 
     pl->launches = 1 + (pl->ngeneric ? 1 : 0);
