@@ -79,7 +79,7 @@ struct msa_server {
     uint32_t max_jobs = 64, quantum = 0;
     double t0 = 0;
     // launch resources (worker thread only)
-    msa::DevBuf bound, tasks, views, counter;
+    msa::DevBuf bound, tasks, views, counter, tasks2, views2, counter2;
     uint64_t bound_stride = 0, grid = 0;
     std::vector<uint32_t> h_tasks;
     std::vector<uint8_t> h_views;
@@ -183,13 +183,105 @@ void release_job_device(Job *j)
     j->mem.release();
 }
 
+// One launch in flight: its completion event and the tasks it took per job.
+struct InFlight {
+    cudaEvent_t done = nullptr;
+    std::vector<std::pair<Job *, uint64_t>> work;
+    bool busy = false;
+    // Pinned staging for this slot's task list and job table (rewritten only
+    // after the slot's previous launch, which consumed them, has retired).
+    void *h_tasks = nullptr, *h_views = nullptr;
+    size_t tasks_cap = 0, views_cap = 0;
+    bool stage(size_t tb, size_t vbytes)
+    {
+        if(tb > tasks_cap) {
+            if(h_tasks) cudaFreeHost(h_tasks);
+            tasks_cap = std::max(tb, tasks_cap * 2);
+            if(cudaMallocHost(&h_tasks, tasks_cap) != cudaSuccess) { h_tasks = nullptr; tasks_cap = 0; return false; }
+        }
+        if(vbytes > views_cap) {
+            if(h_views) cudaFreeHost(h_views);
+            views_cap = std::max(vbytes, views_cap * 2);
+            if(cudaMallocHost(&h_views, views_cap) != cudaSuccess) { h_views = nullptr; views_cap = 0; return false; }
+        }
+        return true;
+    }
+    void release()
+    {
+        if(h_tasks) cudaFreeHost(h_tasks);
+        if(h_views) cudaFreeHost(h_views);
+        h_tasks = h_views = nullptr;
+        tasks_cap = views_cap = 0;
+    }
+};
+
+// Estimated cells of task (rows pair k, group g) of a job.
+static uint64_t task_cells(const Job *j, uint32_t k, uint32_t g)
+{
+    const SeqStore *st = j->st;
+    const uint32_t nclean = (uint32_t) st->clean_sorted.size();
+    const uint64_t e1 = st->eff[st->clean_sorted[2 * k]];
+    const uint32_t b0 = 2 * k + 1 + g * kServeTiles.W;
+    const uint32_t bn = std::min<uint32_t>(nclean, b0 + kServeTiles.W);
+    const uint64_t c0 = b0 < nclean ? st->eff[st->clean_sorted[b0]] : 0;
+    return 2 * e1 * c0 * (bn > b0 ? bn - b0 : 0);
+}
+
 void worker_loop(msa_server *srv)
 {
     msa_ctx *ctx = srv->ctx;
     cudaSetDevice(ctx->device);
+    cudaStream_t compute = ctx->own_stream, upload = nullptr;
+    cudaStreamCreateWithFlags(&upload, cudaStreamNonBlocking);
+    cudaEvent_t uploaded = nullptr;
+    cudaEventCreateWithFlags(&uploaded, cudaEventDisableTiming);
+    InFlight slots[2];
+    for(auto &f : slots) cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming);
+    int cur = 0;
+    const size_t vb = job_view_bytes();
+
+    // Applies a completed launch: counts its tasks and finishes jobs whose
+    // last task ran (scores copied out, device memory released, completion
+    // published under the lock).
+    auto retire = [&](InFlight &f) {
+        if(!f.busy) return;
+        const cudaError_t e = cudaEventSynchronize(f.done);
+        std::vector<Job *> finished;
+        for(auto &w : f.work) {
+            Job *j = w.first;
+            j->finished += w.second;
+            if(e) j->status = MSA_ERR_CUDA;
+            if(j->finished >= j->total_tasks && !j->done) {
+                if(!e && j->status == MSA_OK) {
+                    const uint64_t npairs = (uint64_t) j->n * (j->n - 1) / 2;
+                    cudaError_t e2 = cudaMemcpyAsync(j->result.data(), j->d_out, npairs * 4, cudaMemcpyDeviceToHost, upload);
+                    if(!e2) e2 = cudaStreamSynchronize(upload);
+                    if(e2) j->status = cuda_error(ctx, e2, "job scores to host");
+                }
+                j->t_done = now_ms();
+                release_job_device(j);
+                finished.push_back(j);
+            }
+        }
+        if(e) cuda_error(ctx, e, "serving launch");
+        f.work.clear();
+        f.busy = false;
+        if(!finished.empty()) {
+            std::lock_guard<std::mutex> lk(srv->mu);
+            auto &adm = srv->admitted;
+            for(Job *j : finished) {
+                srv->used -= j->device_bytes;
+                adm.erase(std::find(adm.begin(), adm.end(), j));
+                j->done = true;
+            }
+            srv->cv_done.notify_all();
+        }
+    };
+
     for(;;) {
-        // 1. Admission.
+        // 1. Admission on the upload stream (does not wait for launches in flight).
         std::vector<Job *> to_admit;
+        bool idle = false;
         {
             std::unique_lock<std::mutex> lk(srv->mu);
             if(srv->stop) break;
@@ -202,120 +294,119 @@ void worker_loop(msa_server *srv)
                 srv->used += need;
                 to_admit.push_back(j);
             }
-            if(to_admit.empty() && srv->admitted.empty()) {
+            idle = to_admit.empty() && srv->admitted.empty() && !slots[0].busy && !slots[1].busy;
+            if(idle) {
                 srv->cv_work.wait_for(lk, std::chrono::milliseconds(20));
                 continue;
             }
         }
-        for(Job *j : to_admit) {
-            bool completed = false;
-            const int rc = admit_one(srv, j, &completed);
-            if(rc || completed) {
-                if(rc) { j->status = rc; j->t_done = now_ms(); }
-                release_job_device(j);
+        if(!to_admit.empty()) {
+            ctx->stream = upload;
+            for(Job *j : to_admit) {
+                bool completed = false;
+                const int rc = admit_one(srv, j, &completed);
+                if(rc || completed) {
+                    if(rc) { j->status = rc; j->t_done = now_ms(); }
+                    release_job_device(j);
+                }
+                std::lock_guard<std::mutex> lk(srv->mu);
+                if(rc || completed) {
+                    srv->used -= j->device_bytes;
+                    j->done = true;
+                    srv->cv_done.notify_all();
+                } else {
+                    srv->admitted.push_back(j);
+                }
             }
-            std::lock_guard<std::mutex> lk(srv->mu);
-            if(rc || completed) {
-                srv->used -= j->device_bytes;
-                j->done = true;
-                srv->cv_done.notify_all();
-            } else {
-                srv->admitted.push_back(j);
-            }
+            ctx->stream = compute;
+            cudaEventRecord(uploaded, upload);
+            cudaStreamWaitEvent(compute, uploaded, 0);
         }
+
+        // 2. Retire the launch that used this slot two rounds ago.
+        retire(slots[cur]);
+
         std::vector<Job *> active;
         {
             std::lock_guard<std::mutex> lk(srv->mu);
             for(Job *j : srv->admitted) if(j->issued < j->total_tasks) active.push_back(j);
         }
-        if(active.empty()) continue;
+        if(active.empty()) {
+            retire(slots[cur ^ 1]);
+            continue;
+        }
 
-        // 2. One merged launch: column groups round-robin over the admitted jobs.
+        // 3. Build one merged launch: an equal share of the cell budget per job,
+        // tasks taken round-robin in each job's cost order, then sorted longest
+        // first so the launch's tail holds its smallest tasks.
         uint64_t max_cols = 1;
         for(Job *j : active) for(uint32_t i = 0; i < j->n; ++i) max_cols = std::max<uint64_t>(max_cols, j->st->plen[i]);
         const uint64_t stride = round_up(max_cols + 160, 32);
         if(!srv->grid && serve_grid(ctx, &srv->grid)) break;
         if(stride > srv->bound_stride) {
-            if(srv->bound.ensure(srv->grid * kServeTiles.W * stride * 4)) break;
-            srv->bound_stride = stride;
+            retire(slots[cur ^ 1]);   // the buffer is about to move
+            if(srv->bound.ensure(srv->grid * kServeTiles.W * std::max<uint64_t>(stride, 2048 + 160) * 4)) break;
+            srv->bound_stride = std::max<uint64_t>(stride, 2048 + 160);
         }
-        const uint64_t quantum = srv->quantum ? srv->quantum : 4 * srv->grid;
-        srv->h_tasks.clear();
-        const size_t vb = job_view_bytes();
+        const uint64_t budget_cells = srv->quantum ? (uint64_t) srv->quantum * 1000000ull : 40000000000ull;
+        const uint64_t share = std::max<uint64_t>(budget_cells / active.size(), 1);
+        struct T { uint32_t slot, k, g; uint64_t cost; };
+        std::vector<T> tasks;
+        InFlight &f = slots[cur];
+        f.work.clear();
         srv->h_views.assign(active.size() * vb, 0);
-        std::vector<uint64_t> taken(active.size(), 0);
-        for(size_t s = 0; s < active.size(); ++s)
-            fill_job_view(srv->h_views.data() + s * vb, active[s]->st, active[s]->d_prof, active[s]->d_narrow,
-                          active[s]->d_out, active[s]->ext.penalty);
-        bool any = true;
-        while(srv->h_tasks.size() / 4 < quantum && any) {
-            any = false;
-            for(size_t s = 0; s < active.size() && srv->h_tasks.size() / 4 < quantum; ++s) {
-                Job *j = active[s];
-                if(j->issued + taken[s] >= j->total_tasks) continue;
-                // advance the job's cursor to its next (rows pair, group)
+        for(size_t sl = 0; sl < active.size(); ++sl) {
+            Job *j = active[sl];
+            fill_job_view(srv->h_views.data() + sl * vb, j->st, j->d_prof, j->d_narrow, j->d_out, j->ext.penalty);
+            uint64_t taken = 0, cells = 0;
+            while(j->issued + taken < j->total_tasks && cells < share) {
                 while(j->cur_k < j->groups.size() && j->cur_g >= j->groups[j->cur_k]) { ++j->cur_k; j->cur_g = 0; }
-                srv->h_tasks.push_back((uint32_t) s);
-                srv->h_tasks.push_back(j->cur_k);
-                srv->h_tasks.push_back(j->cur_g);
-                srv->h_tasks.push_back(0);
+                const uint64_t c = task_cells(j, j->cur_k, j->cur_g);
+                tasks.push_back({(uint32_t) sl, j->cur_k, j->cur_g, c});
+                cells += c;
                 ++j->cur_g;
-                ++taken[s];
-                any = true;
+                ++taken;
             }
+            j->issued += taken;
+            if(taken) { f.work.push_back({j, taken}); ++j->launches; }
         }
-        const uint64_t ntasks = srv->h_tasks.size() / 4;
-        cudaError_t e = srv->tasks.ensure(ntasks * 16 + 16);
-        if(!e) e = srv->views.ensure(srv->h_views.size() + 16);
-        if(!e) e = srv->counter.ensure(64);
-        if(!e) e = cudaMemcpyAsync(srv->tasks.ptr, srv->h_tasks.data(), ntasks * 16, cudaMemcpyHostToDevice, ctx->stream);
-        if(!e) e = cudaMemcpyAsync(srv->views.ptr, srv->h_views.data(), srv->h_views.size(), cudaMemcpyHostToDevice,
-                                   ctx->stream);
-        if(!e) e = cudaMemsetAsync(srv->counter.ptr, 0, 64, ctx->stream);
+        std::stable_sort(tasks.begin(), tasks.end(), [](const T &a, const T &b) { return a.cost > b.cost; });
+        const uint64_t ntasks = tasks.size();
+        if(!f.stage(ntasks * 16 + 16, srv->h_views.size() + 16)) { cuda_error(ctx, cudaErrorMemoryAllocation, "pinned staging"); break; }
+        uint32_t *ht = (uint32_t *) f.h_tasks;
+        for(size_t q = 0; q < tasks.size(); ++q) {
+            ht[4 * q] = tasks[q].slot;
+            ht[4 * q + 1] = tasks[q].k;
+            ht[4 * q + 2] = tasks[q].g;
+            ht[4 * q + 3] = 0;
+        }
+        std::memcpy(f.h_views, srv->h_views.data(), srv->h_views.size());
+        // Device buffers of this slot: grow only while nothing else is in flight.
+        DevBuf &tb = cur ? srv->tasks : srv->tasks2, &vbuf = cur ? srv->views : srv->views2,
+               &cb = cur ? srv->counter : srv->counter2;
+        if(tb.bytes < ntasks * 16 + 16 || vbuf.bytes < srv->h_views.size() + 16) retire(slots[cur ^ 1]);
+        cudaError_t e = tb.ensure(std::max<size_t>(ntasks * 16 + 16, 1 << 20));
+        if(!e) e = vbuf.ensure(std::max<size_t>(srv->h_views.size() + 16, 64 << 10));
+        if(!e) e = cb.ensure(64);
+        if(!e) e = cudaMemcpyAsync(tb.ptr, f.h_tasks, ntasks * 16, cudaMemcpyHostToDevice, compute);
+        if(!e) e = cudaMemcpyAsync(vbuf.ptr, f.h_views, srv->h_views.size(), cudaMemcpyHostToDevice, compute);
+        if(!e) e = cudaMemsetAsync(cb.ptr, 0, 64, compute);
         if(!e) {
-            ServeLaunch L{srv->views.ptr, srv->tasks.ptr, ntasks, (uint32_t *) srv->bound.ptr, srv->bound_stride,
-                          (unsigned long long *) srv->counter.ptr};
-            e = launch_serve(L, srv->grid, ctx->stream);
+            ServeLaunch L{vbuf.ptr, tb.ptr, ntasks, (uint32_t *) srv->bound.ptr, srv->bound_stride,
+                          (unsigned long long *) cb.ptr};
+            e = launch_serve(L, srv->grid, compute);
             ctx->launches++;
         }
-        if(!e) e = cudaStreamSynchronize(ctx->stream);
-        const bool failed = e != cudaSuccess;
-        if(failed) cuda_error(ctx, e, "serving launch");
-
-        // 3. Account; finish jobs whose last task ran (device memory released
-        // before completion is published under the lock).
-        std::vector<Job *> finished;
-        for(size_t s = 0; s < active.size(); ++s) {
-            Job *j = active[s];
-            j->issued += taken[s];
-            j->finished += taken[s];
-            if(taken[s]) ++j->launches;
-            if(failed) {
-                j->status = MSA_ERR_CUDA;
-            } else if(j->finished >= j->total_tasks) {
-                const uint64_t npairs = (uint64_t) j->n * (j->n - 1) / 2;
-                cudaError_t e2 = cudaMemcpyAsync(j->result.data(), j->d_out, npairs * 4, cudaMemcpyDeviceToHost,
-                                                 ctx->stream);
-                if(!e2) e2 = cudaStreamSynchronize(ctx->stream);
-                j->status = e2 ? cuda_error(ctx, e2, "job scores to host") : MSA_OK;
-            } else {
-                continue;
-            }
-            j->t_done = now_ms();
-            release_job_device(j);
-            finished.push_back(j);
-        }
-        if(!finished.empty()) {
-            std::lock_guard<std::mutex> lk(srv->mu);
-            auto &adm = srv->admitted;
-            for(Job *j : finished) {
-                srv->used -= j->device_bytes;
-                adm.erase(std::find(adm.begin(), adm.end(), j));
-                j->done = true;
-            }
-            srv->cv_done.notify_all();
-        }
+        if(!e) e = cudaEventRecord(f.done, compute);
+        if(e) cuda_error(ctx, e, "serving launch");
+        f.busy = true;
+        cur ^= 1;
     }
+    retire(slots[0]);
+    retire(slots[1]);
+    for(auto &f : slots) { cudaEventDestroy(f.done); f.release(); }
+    cudaEventDestroy(uploaded);
+    cudaStreamDestroy(upload);
     // Stopping: fail what is still queued or admitted.
     std::lock_guard<std::mutex> lk(srv->mu);
     for(Job *j : srv->pending) { j->status = MSA_ERR_QUEUE; j->done = true; }
@@ -442,6 +533,9 @@ int msa_serve_stop(msa_server *srv)
     srv->tasks.release();
     srv->views.release();
     srv->counter.release();
+    srv->tasks2.release();
+    srv->views2.release();
+    srv->counter2.release();
     msa_destroy(srv->ctx);
     delete srv;
     return MSA_OK;
