@@ -217,16 +217,18 @@ typedef enum msa_tri_kind {
  */
 int msa_nj(msa_ctx *ctx, const void *tri, int tri_kind, uint32_t n, msa_otu *out_nodes);
 
-/* Timing of the context's last msa_nj call. Cycle counts are block 0's SM
- * clock cycles by phase: while the whole grid joins (scan, barrier waits,
- * join) and once one block finishes alone (scan, join). */
+/* Timing of the context's last msa_nj call. The joins run on one cluster of
+ * `cluster` CTAs; cycle counts are SM clock cycles by phase, for CTA 0 (scan,
+ * wait for the candidates, join, wait until every CTA has read the joined
+ * rows, writes) and for the CTA that folds each new node's row sum (the fold,
+ * its scan of the new node's row, its wait for the candidates). */
 typedef struct msa_nj_stats {
     double kernel_ms;
     double total_ms;            /* upload, matrix set-up, joins, download */
     uint32_t n;
-    uint32_t grid_joins;
-    uint64_t cycles_scan, cycles_wait, cycles_join;
-    uint64_t cycles_scan_single, cycles_join_single;
+    uint32_t cluster;
+    uint64_t cycles_scan, cycles_wait, cycles_join, cycles_join_wait, cycles_write;
+    uint64_t cycles_fold, cycles_fold_row, cycles_fold_wait;
 } msa_nj_stats;
 int msa_nj_last_stats(const msa_ctx *ctx, msa_nj_stats *out);
 

@@ -62,9 +62,10 @@ class MsaOtu(ctypes.Structure):
 
 class MsaNjStats(ctypes.Structure):
     _fields_ = [("kernel_ms", ctypes.c_double), ("total_ms", ctypes.c_double), ("n", ctypes.c_uint32),
-                ("grid_joins", ctypes.c_uint32), ("cycles_scan", ctypes.c_uint64), ("cycles_wait", ctypes.c_uint64),
-                ("cycles_join", ctypes.c_uint64), ("cycles_scan_single", ctypes.c_uint64),
-                ("cycles_join_single", ctypes.c_uint64)]
+                ("cluster", ctypes.c_uint32), ("cycles_scan", ctypes.c_uint64), ("cycles_wait", ctypes.c_uint64),
+                ("cycles_join", ctypes.c_uint64), ("cycles_join_wait", ctypes.c_uint64), ("cycles_write", ctypes.c_uint64),
+                ("cycles_fold", ctypes.c_uint64), ("cycles_fold_row", ctypes.c_uint64),
+                ("cycles_fold_wait", ctypes.c_uint64)]
 
 
 class MsaServeConfig(ctypes.Structure):

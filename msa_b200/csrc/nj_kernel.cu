@@ -2,22 +2,36 @@
 // njoining::sequential<transform::symmetric>
 // (src/phylogeny/njoining/impl/sequential.cpp:80-346).
 //
-// The reference shrinks a packed symmetric matrix after every join (swap the
-// removed OTU with logical 0, then drop logical 0: src/phylogeny/matrix.cu:359-384,
-// sequential.cpp:210-224). Here the matrix never moves: D is a full n x n
-// float matrix indexed by physical slot, and a logical -> physical permutation
-// reproduces the reference's index order, which is what its first-maximum
-// tie-break scans. Every float and double operation is written out with an
-// explicit rounding intrinsic in the reference's order, so no FMA contraction
-// or reassociation can change a bit.
+// Layout. The reference keeps a packed symmetric matrix and, after every join,
+// swaps the removed OTU y with logical 0 and deletes logical 0
+// (src/phylogeny/matrix.cu:359-384, sequential.cpp:210-224); every index then
+// shifts down by one, which is the order its first-maximum tie-break scans in.
+// Here D is a full n x n float matrix with row pitch P (a multiple of 4) and, at
+// join number t, logical index k lives in physical slot t + k. Deleting logical
+// 0 is the increment of t; the swap is one row and one column copy from slot t
+// into slot t + y. Each row of the logical lower triangle is therefore one
+// contiguous run of memory, read with 16-byte loads.
 //
-// One cooperative launch runs all joins. While many OTUs remain, every block
-// scans a slice of the logical lower triangle (Q = (c-2)*D - S_i - S_j) for its
-// (max Q, first index) candidate, a grid barrier publishes the slices, every
-// block reduces them identically, block 0 applies the join, and a second
-// barrier releases the next scan. Once few OTUs remain, block 0 finishes alone
-// with block-level barriers only. Every grid-barrier wait is bounded: on
-// timeout the kernel raises an error flag and all blocks return.
+// Schedule. One thread-block cluster of K CTAs (16 where the device allows,
+// else fewer) runs every join. Hardware cluster barriers (release/acquire)
+// split a join into phases:
+//   scan   CTAs 0..K-2 search the logical lower triangle for the largest
+//          Q = (c-2) D - S_i - S_j with its first row-major index; each CTA
+//          holds its own copy of S in shared memory;
+//   A      each CTA's candidate is stored into every CTA's shared memory;
+//   join   every CTA reduces the candidates identically and computes the row
+//          update (new distances, new row sums) for all c rows, so the copies
+//          of S stay equal without any exchange;
+//   B      every read of rows x, y and 0 is done;
+//   write  CTAs 0..K-2 write row and column x and copy logical 0 into y, while
+//          the next scan already runs: that scan reads none of those cells
+//          (see `pend` and `moved` in the kernel).
+// The new node's row sum is a serial float fold over the c updates
+// (sequential.cpp:259), the one sequential piece of a join. CTA K-1 computes
+// it while the others scan the next join, skipping the new node's row and
+// column; CTA K-1 then scans that row and column itself. Every float and double
+// operation is written with an explicit rounding intrinsic in the reference's
+// order, so no FMA contraction or reassociation can change a bit.
 #include <algorithm>
 #include <cfloat>
 #include <cmath>
@@ -31,9 +45,18 @@
 namespace msa {
 namespace njdev {
 
+namespace cg = cooperative_groups;
+
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kThreads = 1024;
-constexpr unsigned long long kSpinLimit = 1ull << 24;   // x 64 ns sleeps ~ 1 s
+constexpr int kThreads = 512;
+constexpr int kWarps = kThreads / 32;
+constexpr unsigned kMaxCluster = 16;
+constexpr uint32_t kNone = 0xffffffffu;
+// Row chunks (4 floats) each lane has in flight while scanning.
+constexpr int kBatch = 16;
+// Phase counters: CTA 0 (scan, wait at A, join, wait at B, writes) and the
+// folding CTA (fold, scan of the new node's row, wait at A).
+constexpr int kCycleSlots = 8;
 
 // Orderable key of a finite or +inf Q value; 0 for NaN and -inf, which the
 // reference's strict `q > best` (best starting at -inf) never selects.
@@ -47,7 +70,7 @@ __device__ __forceinline__ uint32_t order_key(float q)
 }
 
 // Larger Q wins; on equal Q the smaller row-major index (earlier in the
-// reference's scan) wins.
+// reference's scan) wins. 0 means "no candidate".
 __device__ __forceinline__ unsigned long long pack(uint32_t key, uint32_t lin)
 {
     return key ? (((unsigned long long) key << 32) | (0xffffffffu - lin)) : 0ull;
@@ -62,291 +85,390 @@ __device__ __forceinline__ unsigned long long warp_max(unsigned long long v)
     return v;
 }
 
+__device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
+__device__ __forceinline__ void cluster_wait() { asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory"); }
+
 struct State {
-    float *D;                // n x n, physical slots
-    float *S;                // row sums by physical slot
-    uint32_t *perm[2];       // logical -> physical, double buffered
-    uint32_t *map;           // OTU id by physical slot
-    unsigned long long *partial;
-    uint32_t *rec_x, *rec_y; // OTU ids joined at each step
+    float *D;                  // n rows of P floats; slot t + k holds logical k
+    const float *S0;           // initial row sums by slot
+    uint32_t *rec_x, *rec_y;   // logical indices joined at each step
     float *rec_dx, *rec_dy;
-    unsigned *bar;
     int *err;
-    unsigned long long *cycles;   // 6 phase counters written by block 0
-    uint32_t n;
-    uint32_t single_c;       // block 0 continues alone once c <= single_c
+    unsigned long long *cycles;   // kCycleSlots phase counters
+    uint32_t n, P;
 };
 
-__device__ __forceinline__ bool grid_sync(unsigned *bar, unsigned nblocks, unsigned &epoch, int *err)
+__global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
 {
-    __syncthreads();
-    if(threadIdx.x == 0) {
-        ++epoch;
-        __threadfence();
-        atomicAdd(bar, 1u);
-        const unsigned target = epoch * nblocks;
-        unsigned long long spins = 0;
-        for(;;) {
-            unsigned v;
-            asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(bar) : "memory");
-            if(v >= target) break;
-            if(*(volatile int *) err) break;
-            if(++spins > kSpinLimit) { atomicExch(err, 1); break; }
-            __nanosleep(20);
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    return *(volatile int *) err == 0;
-}
-
-// Row-major lower-triangle index -> (i, j), i > j.
-__device__ __forceinline__ void tri_decode(uint64_t L, uint32_t &i, uint32_t &j)
-{
-    uint64_t r = (uint64_t) ((1.0 + sqrt(1.0 + 8.0 * (double) L)) * 0.5);
-    while(r * (r - 1) / 2 > L) --r;
-    while((r + 1) * r / 2 <= L) ++r;
-    i = (uint32_t) r;
-    j = (uint32_t) (L - r * (r - 1) / 2);
-}
-
-// Best (Q, row-major index) of rows gw, gw + nwt, ... of the logical lower
-// triangle. kCG: other blocks write D, so loads bypass L1.
-template <bool kCG>
-__device__ __forceinline__ void scan_rows(const float *__restrict__ D, uint32_t n, const uint32_t *pl, const float *Sl,
-                                          uint32_t c, float cm2, uint32_t gw, uint32_t nwt, int lane, float &bq,
-                                          uint32_t &bl)
-{
-    for(uint32_t i = 1 + gw; i < c; i += nwt) {
-        const float *row = D + (size_t) pl[i] * n;
-        const float si = Sl[i];
-        const uint32_t base = i * (i - 1) / 2;
-        for(uint32_t j = lane; j < i; j += 32) {
-            const float d = kCG ? __ldcg(row + pl[j]) : row[pl[j]];
-            const float q = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d), si), Sl[j]);
-            if(q > bq) { bq = q; bl = base + j; }
-        }
-    }
-}
-
-__global__ void __launch_bounds__(kThreads) nj_kernel(State st)
-{
+    cg::cluster_group cluster = cg::this_cluster();
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const uint32_t n = st.n;
-    // Shared layout (16-byte aligned regions): logical -> physical slots, S in
-    // logical order (reused for the float row-sum updates once a join has read
-    // it), and block 0's double-precision updates.
-    const size_t off_s = ((size_t) n * 4 + 15) & ~(size_t) 15;
-    const size_t off_u = (off_s + (size_t) n * 4 + 15) & ~(size_t) 15;
-    uint32_t *pl = reinterpret_cast<uint32_t *>(smem_raw);
-    float *Sl = reinterpret_cast<float *>(smem_raw + off_s);
-    double *upd = reinterpret_cast<double *>(smem_raw + off_u);
-    __shared__ unsigned long long wbest[kThreads / 32];
-    __shared__ unsigned long long chosen;
-    __shared__ uint8_t exact_all;
+    const uint32_t n = st.n, P = st.P;
+    // Shared layout: S by slot, new distances ND and double updates U by
+    // logical index (all P entries long; P is a multiple of 4).
+    float *S = reinterpret_cast<float *>(smem_raw);
+    float *ND = S + P;
+    double *U = reinterpret_cast<double *>(smem_raw + (size_t) 8 * P);
+    __shared__ unsigned long long parts[kMaxCluster];   // each CTA's candidate
+    __shared__ uint32_t part_xy[kMaxCluster];           // and its (x << 16 | y)
+    __shared__ unsigned long long wbest[kWarps];
+    __shared__ uint32_t wxy[kWarps];
+    // Phase cycle counters live in shared memory, leaving registers to the
+    // scan's loads in flight.
+    __shared__ unsigned long long cyc[kCycleSlots];
 
-    const unsigned nblocks = gridDim.x;
+    const unsigned K = cluster.num_blocks();
+    const unsigned rank = cluster.block_rank();
+    const unsigned F = K - 1;   // the CTA that folds new row sums
+    const bool folder = rank == F;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    unsigned epoch = 0;
-    // Block 0, thread 0: cycles spent per phase (grid: scan, wait, join, wait;
-    // single: scan, join) for msa_nj_last_stats.
-    unsigned long long cyc[6] = {0, 0, 0, 0, 0, 0};
+    float *D = st.D;
+    const bool timer = tid == 0 && (rank == 0 || folder);
+    if(tid < kCycleSlots) cyc[tid] = 0;
     unsigned long long t_last = clock64();
     auto mark = [&](int k) {
-        const unsigned long long t = clock64();
-        cyc[k] += t - t_last;
-        t_last = t;
+        const unsigned long long now = clock64();
+        cyc[k] += now - t_last;
+        t_last = now;
     };
-    uint32_t c = n;
-    int buf = 0;
-    uint32_t next_parent = n;
-    uint32_t step = 0;
+
+    for(uint32_t k = tid; k < P; k += kThreads) {
+        S[k] = k < n ? st.S0[k] : 0.0f;
+        ND[k] = 0.0f;
+    }
+    cluster.sync();   // every CTA is running before any shared-memory exchange
+
+    uint32_t c = n, t = 0, step = 0;
+    // Logical indices (in the current window) that the previous join left
+    // unfinished: `pend` is the new node, whose row sum CTA F is still folding
+    // and whose row and column only CTA F scans (from ND); `moved` took logical
+    // 0's data, which the previous join's writes may not have copied yet, so
+    // scans read it where it was (slot t - 1): its row there, and column t - 1
+    // of every later row.
+    uint32_t pend = kNone, moved = kNone;
+    bool failed = false;
 
     while(c > 1) {
-        const bool single = c <= st.single_c;
-        if(single && blockIdx.x != 0) return;
-        const uint32_t *perm = buf ? st.perm[1] : st.perm[0];
-
-        for(uint32_t k = tid; k < c; k += kThreads) {
-            const uint32_t p = __ldcg(perm + k);
-            pl[k] = p;
-            Sl[k] = __ldcg(st.S + p);
-        }
-        __syncthreads();
-
-        // ---- scan: warps take rows i = 1..c-1 round-robin; lanes stride over
-        // j < i. Each thread visits its pairs in increasing row-major index, so
-        // a strict `>` keeps its first maximum, as the reference's scan does.
         const float cm2 = (float) (c - 2);
-        const uint32_t nwt = (single ? 1u : nblocks) * (kThreads / 32);
-        const uint32_t gw = (single ? 0u : blockIdx.x) * (kThreads / 32) + warp;
-        float bq = -INFINITY;
-        uint32_t bl = 0;
-        if(single) scan_rows<false>(st.D, n, pl, Sl, c, cm2, gw, nwt, lane, bq, bl);
-        else scan_rows<true>(st.D, n, pl, Sl, c, cm2, gw, nwt, lane, bq, bl);
-        unsigned long long best = pack(order_key(bq), bl);
-        if(blockIdx.x == 0 && tid == 0) mark(single ? 4 : 0);
-        best = warp_max(best);
-        if(lane == 0) wbest[warp] = best;
+        unsigned long long best = 0;
+        uint32_t best_xy = 0;
+        auto offer = [&](unsigned long long v, uint32_t i, uint32_t j) {
+            if(v > best) {
+                best = v;
+                best_xy = (i << 16) | j;
+            }
+        };
+
+        // ---- scan
+        if(!folder) {
+            // Rows i = 1..c-1 of the logical lower triangle; warp w takes rows
+            // w and 2W-1-w of every 2W, so a long and a short row pair up, and
+            // loads the pair's chunks kBatch at a time per lane.
+            const uint32_t W = F * kWarps;
+            const uint32_t gw = rank * kWarps + warp;
+            const uint32_t skip1 = pend == kNone ? kNone : t + pend;
+            const uint32_t skip2 = moved == kNone ? kNone : t + moved;
+            const uint32_t base4 = t & ~3u;
+            const float s_moved = moved == kNone ? 0.0f : S[t + moved];
+            auto chunk = [&](const float4 &d, uint32_t col, uint32_t hi, float si, float &bq, uint32_t &bc) {
+                const float4 s = *reinterpret_cast<const float4 *>(S + col);
+                const float q0 = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d.x), si), s.x);
+                const float q1 = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d.y), si), s.y);
+                const float q2 = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d.z), si), s.z);
+                const float q3 = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d.w), si), s.w);
+                if(col >= t && col + 4 <= hi && skip1 - col >= 4u && skip2 - col >= 4u) {
+                    if(q0 > bq) { bq = q0; bc = col; }
+                    if(q1 > bq) { bq = q1; bc = col + 1; }
+                    if(q2 > bq) { bq = q2; bc = col + 2; }
+                    if(q3 > bq) { bq = q3; bc = col + 3; }
+                } else {
+                    auto ok = [&](uint32_t k) { return k >= t && k < hi && k != skip1 && k != skip2; };
+                    if(ok(col) && q0 > bq) { bq = q0; bc = col; }
+                    if(ok(col + 1) && q1 > bq) { bq = q1; bc = col + 1; }
+                    if(ok(col + 2) && q2 > bq) { bq = q2; bc = col + 2; }
+                    if(ok(col + 3) && q3 > bq) { bq = q3; bc = col + 3; }
+                }
+            };
+            for(uint32_t base = 0; base + 1 < c; base += 2 * W) {
+                uint32_t ia = base + 1 + gw, ib = base + 2 * W - gw;
+                if(ia >= c || ia == pend) ia = kNone;
+                if(ib >= c || ib == pend) ib = kNone;
+                const uint32_t na = ia == kNone ? 0 : (t + ia - base4 + 3) >> 2;
+                const uint32_t nb = ib == kNone ? 0 : (t + ib - base4 + 3) >> 2;
+                const float *rowa = D + (size_t) (ia == kNone ? t : ia == moved ? t - 1 : t + ia) * P + base4;
+                const float *rowb = D + (size_t) (ib == kNone ? t : ib == moved ? t - 1 : t + ib) * P + base4;
+                // Column `moved` of a later row: lane 0 for row a, lane 1 for row b.
+                const uint32_t ir = lane == 0 ? ia : ib;
+                const bool redirect = lane < 2 && moved != kNone && ir != kNone && ir > moved;
+                const float dm = redirect ? __ldcg(D + (size_t) (t + ir) * P + t - 1) : 0.0f;
+                const float sa = ia == kNone ? 0.0f : S[t + ia], sb = ib == kNone ? 0.0f : S[t + ib];
+                float bqa = -INFINITY, bqb = -INFINITY;
+                uint32_t bca = 0, bcb = 0;
+                for(uint32_t g0 = 0; g0 < na + nb; g0 += 32 * kBatch) {
+                    float4 d[kBatch];
+#pragma unroll
+                    for(int u = 0; u < kBatch; ++u) {
+                        const uint32_t g = g0 + lane + 32 * u;
+                        if(g < na) d[u] = __ldcg(reinterpret_cast<const float4 *>(rowa + 4 * g));
+                        else if(g < na + nb) d[u] = __ldcg(reinterpret_cast<const float4 *>(rowb + 4 * (g - na)));
+                    }
+#pragma unroll
+                    for(int u = 0; u < kBatch; ++u) {
+                        const uint32_t g = g0 + lane + 32 * u;
+                        if(g < na) chunk(d[u], base4 + 4 * g, t + ia, sa, bqa, bca);
+                        else if(g < na + nb) chunk(d[u], base4 + 4 * (g - na), t + ib, sb, bqb, bcb);
+                    }
+                }
+                if(ia != kNone && order_key(bqa)) offer(pack(order_key(bqa), ia * (ia - 1) / 2 + (bca - t)), ia, bca - t);
+                if(ib != kNone && order_key(bqb)) offer(pack(order_key(bqb), ib * (ib - 1) / 2 + (bcb - t)), ib, bcb - t);
+                if(redirect) {
+                    const float q = __fsub_rn(__fsub_rn(__fmul_rn(cm2, dm), lane == 0 ? sa : sb), s_moved);
+                    offer(pack(order_key(q), ir * (ir - 1) / 2 + moved), ir, moved);
+                }
+            }
+        } else if(pend != kNone) {
+            // The new node's row and column, from the distances the last join
+            // computed (ND, indexed by that join's logical order): pairs
+            // (pend, j < pend) and (j > pend, pend) with the reference's
+            // operand order for each.
+            const uint32_t x = pend;
+            const float sx = S[t + x];
+            for(uint32_t j = tid; j < c; j += kThreads) {
+                if(j == x) continue;
+                const float d = ND[j == moved ? 0 : j + 1];
+                const float sj = S[t + j];
+                if(j < x) {
+                    const float q = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d), sx), sj);
+                    offer(pack(order_key(q), x * (x - 1) / 2 + j), x, j);
+                } else {
+                    const float q = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d), sj), sx);
+                    offer(pack(order_key(q), j * (j - 1) / 2 + x), j, x);
+                }
+            }
+        }
+        // Candidates are unique (distinct indices), so the holder of the
+        // maximum also names its (x, y).
+        {
+            const unsigned long long wm = warp_max(best);
+            if(best == wm && wm != 0ull) wxy[warp] = best_xy;
+            if(lane == 0) wbest[warp] = wm;
+        }
         __syncthreads();
         if(warp == 0) {
-            unsigned long long v = wbest[lane];
-            v = warp_max(v);
-            if(lane == 0) {
-                if(single) chosen = v;
-                else __stcg(st.partial + blockIdx.x, v);
+            const unsigned long long v = lane < kWarps ? wbest[lane] : 0ull;
+            const unsigned long long m = warp_max(v);
+            const uint32_t holder = __ffs(__ballot_sync(kFull, v == m)) - 1;
+            const uint32_t xy = m ? wxy[holder] : 0u;
+            if((unsigned) lane < K) {
+                cluster.map_shared_rank(parts, (unsigned) lane)[rank] = m;
+                cluster.map_shared_rank(part_xy, (unsigned) lane)[rank] = xy;
             }
         }
-        if(!single) {
-            if(!grid_sync(st.bar, nblocks, epoch, st.err)) return;
-            if(blockIdx.x == 0 && tid == 0) mark(1);
-            if(warp == 0) {
-                unsigned long long v = 0;
-                for(unsigned b = lane; b < nblocks; b += 32) v = umax64(v, __ldcg(st.partial + b));
-                v = warp_max(v);
-                if(lane == 0) chosen = v;
+        if(timer) mark(rank == 0 ? 0 : 6);
+        cluster_arrive();   // A
+        cluster_wait();
+        if(timer) mark(rank == 0 ? 1 : 7);
+
+        // ---- join
+        unsigned long long win = 0;
+        unsigned wr = 0;
+        for(unsigned r = 0; r < K; ++r)
+            if(parts[r] > win) {
+                win = parts[r];
+                wr = r;
             }
-        }
-        __syncthreads();
-        const unsigned long long win = chosen;
         if(win == 0ull) {   // no selectable Q (all NaN): the reference would index an undefined pair
-            if(tid == 0) atomicExch(st.err, 2);
-            return;
+            failed = true;
+            break;
         }
+        const uint32_t x = part_xy[wr] >> 16, y = part_xy[wr] & 0xffffu;
+        const float *rx = D + (size_t) (t + x) * P + t;
+        const float *ry = D + (size_t) (t + y) * P + t;
+        const float *r0 = D + (size_t) t * P + t;
+        const float dxy = __ldcg(rx + y);
+        // This thread's first element of the write slice (CTAs 0..F-1):
+        // logical 0's entry, loaded now so the writes wait for no load.
+        const uint32_t wlo = folder ? 0 : (uint32_t) ((uint64_t) c * rank / F);
+        const uint32_t whi = folder ? 0 : (uint32_t) ((uint64_t) c * (rank + 1) / F);
+        const uint32_t wi = wlo + tid;
+        const float v0 = (wi < whi && y != 0) ? __ldcg(r0 + wi) : 0.0f;
 
-        // ---- join (block 0 only; the others wait at the next barrier).
-        if(blockIdx.x == 0) {
-            const uint32_t lin = 0xffffffffu - (uint32_t) (win & 0xffffffffull);
-            uint32_t x, y;
-            tri_decode(lin, x, y);
-            const uint32_t px = pl[x], py = pl[y];
-            const float dxy = __ldcg(st.D + (size_t) px * n + py);
+        // raise_candidate (sequential.cpp:142-152) and the join record.
+        if(rank == 0 && tid == 0) {
+            const float pairsum = __fsub_rn(S[t + x], S[t + y]);
+            const float den = (float) (2u * (c - 2));
+            const float q = __fdiv_rn(pairsum, den);
+            float dx = __double2float_rn(__dadd_rn(__dmul_rn(0.5, (double) dxy), (double) q));
+            float dy = __fsub_rn(dxy, dx);
+            // The last join divides by 2(c-2) = 0; for 0/0 the reference's x86
+            // SSE arithmetic yields the default NaN 0xFFC00000 and propagates it
+            // into dx and dy, where the GPU would give its canonical 0x7FFFFFFF.
+            if(dx != dx) dx = __uint_as_float(0xFFC00000u);
+            if(dy != dy) dy = __uint_as_float(0xFFC00000u);
+            st.rec_x[step] = x;
+            st.rec_y[step] = y;
+            st.rec_dx[step] = dx;
+            st.rec_dy[step] = dy;
+        }
+        __syncthreads();   // S[x], S[y] are read before the row sums change
 
-            // raise_candidate (sequential.cpp:142-152).
-            if(tid == 0) {
-                const float pairsum = __fsub_rn(Sl[x], Sl[y]);
-                const float den = (float) (2u * (c - 2));
-                const float q = __fdiv_rn(pairsum, den);
-                float dx = __double2float_rn(__dadd_rn(__dmul_rn(0.5, (double) dxy), (double) q));
-                float dy = __fsub_rn(dxy, dx);
-                // The last join divides by 2(c-2) = 0; for 0/0 the reference's x86
-                // SSE arithmetic yields the default NaN 0xFFC00000 and propagates it
-                // into dx and dy, where the GPU would give its canonical 0x7FFFFFFF.
-                if(dx != dx) dx = __uint_as_float(0xFFC00000u);
-                if(dy != dy) dy = __uint_as_float(0xFFC00000u);
-                st.rec_x[step] = __ldcg(st.map + px);
-                st.rec_y[step] = __ldcg(st.map + py);
-                st.rec_dx[step] = dx;
-                st.rec_dy[step] = dy;
-                exact_all = 1;
-            }
-            __syncthreads();
-
-            // join_pair (sequential.cpp:247-267): per-row updates.
-            bool exact = true;
-            for(uint32_t i = tid; i < c; i += kThreads) {
-                const uint32_t p = pl[i];
-                float a, b;
-                if(i == x) { a = __ldcg(st.D + (size_t) px * n + px); b = dxy; }
-                else if(i == y) { a = dxy; b = __ldcg(st.D + (size_t) py * n + py); }
-                else { a = __ldcg(st.D + (size_t) p * n + px); b = __ldcg(st.D + (size_t) p * n + py); }
+        // join_pair (sequential.cpp:247-267). D[i][x] and D[i][y] are read as
+        // row x and row y (the matrix is symmetric bit for bit); i = x and
+        // i = y read the diagonal and D[x][y], as the reference does.
+        bool exact = true;
+        {
+            uint32_t i = tid;
+            float a = i < c ? __ldcg(rx + i) : 0.0f, b = i < c ? __ldcg(ry + i) : 0.0f;
+            for(; i < c; i += kThreads) {
+                const uint32_t in = i + kThreads;
+                const float an = in < c ? __ldcg(rx + in) : 0.0f, bn = in < c ? __ldcg(ry + in) : 0.0f;
                 const float prev = __fadd_rn(a, b);
                 const double u = __dmul_rn((double) __fsub_rn(prev, dxy), 0.5);
-                upd[i] = u;
-                exact = exact && ((double) __double2float_rn(u) == u);
                 const float nd = __double2float_rn(u);
-                __stcg(st.D + (size_t) p * n + px, nd);
-                __stcg(st.D + (size_t) px * n + p, nd);
-                if(i != x) {
-                    const float s = __double2float_rn(__dadd_rn((double) Sl[i], __dsub_rn(u, (double) prev)));
-                    __stcg(st.S + p, s);
-                }
-                Sl[i] = nd;   // this thread's own slot: S[i] was read just above
+                U[i] = u;
+                ND[i] = nd;
+                exact = exact && ((double) nd == u);
+                if(i != x) S[t + i] = __double2float_rn(__dadd_rn((double) S[t + i], __dsub_rn(u, (double) prev)));
+                a = an;
+                b = bn;
             }
-            if(!exact) exact_all = 0;
-            __syncthreads();
+        }
+        exact = __syncthreads_and(exact);
+        // update_cache (sequential.cpp:210-224): logical 0 takes y's place.
+        if(y != 0 && tid == 0) S[t + y] = S[t];
+        if(timer && rank == 0) mark(2);
+        cluster_arrive();   // B: every read of rows x, y and 0 is done
+        cluster_wait();
 
-            // Serial fold of the new row sum (sequential.cpp:259): i ascending.
-            // When every update is a float value, the double add rounded to float
-            // equals a float add (double has >= 2*24+2 significand bits), so the
-            // short-latency float chain is used; otherwise the literal double one.
-            if(tid == 0) {
+        if(folder) {
+            // Serial fold of the new row sum, i ascending. When every update is
+            // a float value, the double add rounded to float equals a float add
+            // (double has >= 2*24+2 significand bits), so the short float chain
+            // is used; otherwise the literal double one. Warp 0 runs it: each
+            // chunk of 32 updates is loaded one per lane (the next chunk while
+            // the current one is added) and handed out by shuffles, and every
+            // lane adds the same chain, so no lane diverges.
+            if(warp == 0) {
+                const unsigned long long f0 = clock64();
                 float ns = 0.0f;
-                if(exact_all) {
-                    // Prefetched float4 batches keep the loads off the add chain.
-                    const float4 *v4 = reinterpret_cast<const float4 *>(Sl);
-                    const uint32_t c4 = c / 4;
-                    float4 a = c4 > 0 ? v4[0] : make_float4(0, 0, 0, 0);
-                    float4 b = c4 > 1 ? v4[1] : make_float4(0, 0, 0, 0);
-                    for(uint32_t q = 0; q < c4; ++q) {
-                        const float4 cur = a;
-                        a = b;
-                        if(q + 2 < c4) b = v4[q + 2];
-                        ns = __fadd_rn(ns, cur.x);
-                        ns = __fadd_rn(ns, cur.y);
-                        ns = __fadd_rn(ns, cur.z);
-                        ns = __fadd_rn(ns, cur.w);
+                if(exact) {
+                    float v = (uint32_t) lane < c ? ND[lane] : 0.0f;
+                    for(uint32_t base = 0; base < c; base += 32) {
+                        const float cur = v;
+                        const uint32_t nxt = base + 32 + lane;
+                        v = nxt < c ? ND[nxt] : 0.0f;
+                        const uint32_t m = min(32u, c - base);
+#pragma unroll
+                        for(int k = 0; k < 32; ++k) {
+                            const float e = __shfl_sync(kFull, cur, k);
+                            if((uint32_t) k < m) ns = __fadd_rn(ns, e);
+                        }
                     }
-                    for(uint32_t i = 4 * c4; i < c; ++i) ns = __fadd_rn(ns, Sl[i]);
                 } else {
-                    for(uint32_t i = 0; i < c; ++i) ns = __double2float_rn(__dadd_rn((double) ns, upd[i]));
+                    for(uint32_t i = 0; i < c; ++i) ns = __double2float_rn(__dadd_rn((double) ns, U[i]));
                 }
-                __stcg(st.S + px, ns);
-                __stcg(st.map + px, next_parent);
-            } else {
-                // update_cache, symmetric (sequential.cpp:210-224): logical 0 and y
-                // swap, then logical 0 is dropped.
-                uint32_t *np = buf ? st.perm[0] : st.perm[1];
-                for(uint32_t k = tid - 1; k + 1 < c; k += kThreads - 1) {
-                    const uint32_t v = (y > 0 && k == y - 1) ? pl[0] : pl[k + 1];
-                    __stcg(np + k, v);
+                if(lane == 0) cyc[5] += clock64() - f0;
+                if((unsigned) lane < K) cluster.map_shared_rank(S, (unsigned) lane)[t + x] = ns;
+            }
+            __syncthreads();   // the folded row sum is in this CTA's S
+            if(timer) t_last = clock64();
+        } else {
+            if(timer) mark(3);
+            // Row/column x get the new distances; logical 0's row/column move
+            // into y.
+            float *wx = D + (size_t) (t + x) * P + t;
+            float *wy = D + (size_t) (t + y) * P + t;
+            for(uint32_t i = wi; i < whi; i += kThreads) {
+                if(i == 0 || i == y) {
+                    if(i == y && y != 0) __stcg(wy + y, __ldcg(r0));   // logical 0's diagonal
+                    continue;
+                }
+                if(i == x) {
+                    __stcg(wx + x, ND[x]);
+                    if(y != 0) {
+                        __stcg(wx + y, ND[0]);
+                        __stcg(wy + x, ND[0]);
+                    }
+                    continue;
+                }
+                const float nd = ND[i];
+                __stcg(wx + i, nd);
+                __stcg(D + (size_t) (t + i) * P + t + x, nd);
+                if(y != 0) {
+                    const float v = i == wi ? v0 : __ldcg(r0 + i);
+                    __stcg(wy + i, v);
+                    __stcg(D + (size_t) (t + i) * P + t + y, v);
                 }
             }
+            if(timer) mark(4);
         }
-        ++next_parent;
+
+        // Logical 0 leaves the window; the new node sits at x - 1 and logical
+        // 0's data at y - 1.
+        pend = x - 1;
+        moved = y != 0 ? y - 1 : kNone;
+        ++t;
         ++step;
-        buf ^= 1;
         --c;
-        if(blockIdx.x == 0 && tid == 0) mark(single ? 5 : 2);
-        if(!single) {
-            if(!grid_sync(st.bar, nblocks, epoch, st.err)) return;
-            if(blockIdx.x == 0 && tid == 0) mark(3);
-        } else {
-            __threadfence_block();
-            __syncthreads();
-        }
     }
-    if(blockIdx.x == 0 && tid == 0)
-        for(int k = 0; k < 6; ++k) st.cycles[k] = cyc[k];
+    if(failed && rank == 0 && tid == 0) atomicExch(st.err, 2);
+    if(tid == 0 && rank == 0)
+        for(int k = 0; k < 5; ++k) st.cycles[k] = cyc[k];
+    if(tid == 0 && folder)
+        for(int k = 5; k < kCycleSlots; ++k) st.cycles[k] = cyc[k];
+    cluster.sync();   // no CTA leaves while another may still write its shared memory
 }
 
-// Packed triangle (float or int32) -> full symmetric matrix, diagonal 0.
+// Packed triangle (float or int32) -> full symmetric matrix of pitch P,
+// diagonal and padding 0.
 template <class T>
-__global__ void inflate_kernel(const T *__restrict__ tri, float *__restrict__ D, uint32_t n)
+__global__ void inflate_kernel(const T *__restrict__ tri, float *__restrict__ D, uint32_t n, uint32_t P)
 {
-    const uint64_t total = (uint64_t) n * n;
+    const uint64_t total = (uint64_t) n * P;
     for(uint64_t e = (uint64_t) blockIdx.x * blockDim.x + threadIdx.x; e < total; e += (uint64_t) gridDim.x * blockDim.x) {
-        const uint64_t i = e / n, j = e - i * n;
+        const uint64_t i = e / P, j = e - i * P;
         float v = 0.0f;
-        if(i > j) v = (float) tri[i * (i - 1) / 2 + j];
-        else if(j > i) v = (float) tri[j * (j - 1) / 2 + i];
+        if(j < n) {
+            if(i > j) v = (float) tri[i * (i - 1) / 2 + j];
+            else if(j > i) v = (float) tri[j * (j - 1) / 2 + i];
+        }
         D[e] = v;
     }
 }
 
 // cache_init (sequential.cpp:80-94): S[k] folds D[k][j] over j != k ascending,
 // from 0. Thread k reads column k (= row k by symmetry) so a warp's reads coalesce.
-__global__ void row_sums_kernel(const float *__restrict__ D, float *__restrict__ S, uint32_t *perm,
-                                uint32_t *map, uint32_t n)
+__global__ void row_sums_kernel(const float *__restrict__ D, float *__restrict__ S, uint32_t n, uint32_t P)
 {
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if(k >= n) return;
     float s = 0.0f;
     for(uint32_t j = 0; j < n; ++j)
-        if(j != k) s = __fadd_rn(s, D[(size_t) j * n + k]);
+        if(j != k) s = __fadd_rn(s, D[(size_t) j * P + k]);
     S[k] = s;
-    perm[k] = k;
-    map[k] = k;
+}
+
+// Largest cluster (16, 8, 4 or 2 CTAs) that can be resident with `smem` bytes
+// of dynamic shared memory per CTA; 0 if none.
+unsigned pick_cluster(size_t smem)
+{
+    for(unsigned k : {16u, 8u, 4u, 2u}) {
+        cudaLaunchConfig_t cfg = {};
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = k;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.gridDim = dim3(k);
+        cfg.blockDim = dim3(kThreads);
+        cfg.dynamicSmemBytes = smem;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int clusters = 0;
+        if(cudaOccupancyMaxActiveClusters(&clusters, nj_cluster_kernel, &cfg) == cudaSuccess && clusters >= 1)
+            return k;
+        cudaGetLastError();
+    }
+    return 0;
 }
 
 }  // namespace njdev
@@ -354,34 +476,36 @@ __global__ void row_sums_kernel(const float *__restrict__ D, float *__restrict__
 int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out)
 {
     cudaStream_t s = ctx->stream;
-    const size_t smem = (size_t) n * 16 + 32;   // pl, Sl (4 B each), upd (8 B), alignment
-    if(smem > 200 * 1024) return set_error(ctx, MSA_ERR_TOO_LARGE, "neighbor-joining supports at most 12800 OTUs");
+    const uint32_t P = (n + 3) & ~3u;
+    const size_t smem = (size_t) P * 16;   // S, ND (4 B each), U (8 B)
+    if(n > 12800) return set_error(ctx, MSA_ERR_TOO_LARGE, "neighbor-joining supports at most 12800 OTUs");
     const uint64_t ntri = (uint64_t) n * (n - 1) / 2;
 
     // Device layout.
     size_t off = 0;
     auto take = [&off](size_t b) { size_t o = off; off = round_up(off + b, 256); return o; };
-    const size_t oD = take((size_t) n * n * 4), oS = take(n * 4), oP0 = take(n * 4), oP1 = take(n * 4),
-                 oM = take(n * 4), oPart = take(4096 * 8), oRx = take(n * 4), oRy = take(n * 4),
-                 oRdx = take(n * 4), oRdy = take(n * 4), oBar = take(64), oErr = take(64), oCyc = take(64),
+    const size_t oD = take((size_t) n * P * 4), oS = take(n * 4), oRx = take(n * 4), oRy = take(n * 4),
+                 oRdx = take(n * 4), oRdy = take(n * 4), oErr = take(64), oCyc = take(64),
                  oTri = take((kind == MSA_TRI_F32_HOST || kind == MSA_TRI_I32_HOST) ? ntri * 4 : 0);
     MSA_CUDA_TRY(ctx, ctx->nj_buf.ensure(off));
     char *base = (char *) ctx->nj_buf.ptr;
     njdev::State st{};
     st.D = (float *) (base + oD);
-    st.S = (float *) (base + oS);
-    st.perm[0] = (uint32_t *) (base + oP0);
-    st.perm[1] = (uint32_t *) (base + oP1);
-    st.map = (uint32_t *) (base + oM);
-    st.partial = (unsigned long long *) (base + oPart);
+    st.S0 = (const float *) (base + oS);
     st.rec_x = (uint32_t *) (base + oRx);
     st.rec_y = (uint32_t *) (base + oRy);
     st.rec_dx = (float *) (base + oRdx);
     st.rec_dy = (float *) (base + oRdy);
-    st.bar = (unsigned *) (base + oBar);
     st.err = (int *) (base + oErr);
     st.cycles = (unsigned long long *) (base + oCyc);
     st.n = n;
+    st.P = P;
+
+    MSA_CUDA_TRY(ctx, cudaFuncSetAttribute(njdev::nj_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                           (int) smem));
+    MSA_CUDA_TRY(ctx, cudaFuncSetAttribute(njdev::nj_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    const unsigned K = njdev::pick_cluster(smem);
+    if(K < 2) return set_error(ctx, MSA_ERR_CUDA, "neighbor-joining cluster cannot be resident");
 
     MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[0], s));
     const void *dtri = tri;
@@ -389,33 +513,35 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out)
         MSA_CUDA_TRY(ctx, cudaMemcpyAsync(base + oTri, tri, ntri * 4, cudaMemcpyHostToDevice, s));
         dtri = base + oTri;
     }
-    const unsigned ib = (unsigned) std::min<uint64_t>(((uint64_t) n * n + 255) / 256, 65535);
+    const unsigned ib = (unsigned) std::min<uint64_t>(((uint64_t) n * P + 255) / 256, 65535);
     if(kind == MSA_TRI_F32_HOST || kind == MSA_TRI_F32_DEVICE)
-        njdev::inflate_kernel<float><<<ib, 256, 0, s>>>((const float *) dtri, st.D, n);
+        njdev::inflate_kernel<float><<<ib, 256, 0, s>>>((const float *) dtri, st.D, n, P);
     else
-        njdev::inflate_kernel<int32_t><<<ib, 256, 0, s>>>((const int32_t *) dtri, st.D, n);
+        njdev::inflate_kernel<int32_t><<<ib, 256, 0, s>>>((const int32_t *) dtri, st.D, n, P);
     MSA_CUDA_TRY(ctx, cudaGetLastError());
-    njdev::row_sums_kernel<<<(n + 255) / 256, 256, 0, s>>>(st.D, st.S, st.perm[0], st.map, n);
+    njdev::row_sums_kernel<<<(n + 255) / 256, 256, 0, s>>>(st.D, (float *) (base + oS), n, P);
     MSA_CUDA_TRY(ctx, cudaGetLastError());
-    MSA_CUDA_TRY(ctx, cudaMemsetAsync(base + oBar, 0, 64, s));
     MSA_CUDA_TRY(ctx, cudaMemsetAsync(base + oErr, 0, 64, s));
+    MSA_CUDA_TRY(ctx, cudaMemsetAsync(base + oCyc, 0, 64, s));
     ctx->launches += 2;
 
-    MSA_CUDA_TRY(ctx, cudaFuncSetAttribute(njdev::nj_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-    int per_sm = 0;
-    MSA_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, njdev::nj_kernel, njdev::kThreads, smem));
-    if(per_sm < 1) return set_error(ctx, MSA_ERR_CUDA, "neighbor-joining kernel cannot be resident");
-    unsigned grid = (unsigned) ctx->num_sms;   // one block per SM; co-resident by cooperative launch
-    // Small problems: one block does everything.
-    st.single_c = 1024;
-    if(n <= st.single_c) grid = 1;
-    void *args[] = {&st};
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = K;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.gridDim = dim3(K);
+    cfg.blockDim = dim3(njdev::kThreads);
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
     MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[1], s));
-    MSA_CUDA_TRY(ctx, cudaLaunchCooperativeKernel((const void *) njdev::nj_kernel, dim3(grid), dim3(njdev::kThreads),
-                                                  args, smem, s));
+    MSA_CUDA_TRY(ctx, cudaLaunchKernelEx(&cfg, njdev::nj_cluster_kernel, st));
     MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[2], s));
     ctx->launches++;
-    unsigned long long cyc[6] = {0, 0, 0, 0, 0, 0};
+    unsigned long long cyc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 
     std::vector<uint32_t> rx(n - 1), ry(n - 1);
     std::vector<float> rdx(n - 1), rdy(n - 1);
@@ -435,27 +561,35 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out)
         ns.kernel_ms = ms;
         ns.total_ms = ms_all;
         ns.n = n;
-        ns.grid_joins = n > st.single_c ? n - st.single_c : 0;
+        ns.cluster = K;
         ns.cycles_scan = cyc[0];
-        ns.cycles_wait = cyc[1] + cyc[3];
+        ns.cycles_wait = cyc[1];
         ns.cycles_join = cyc[2];
-        ns.cycles_scan_single = cyc[4];
-        ns.cycles_join_single = cyc[5];
+        ns.cycles_join_wait = cyc[3];
+        ns.cycles_write = cyc[4];
+        ns.cycles_fold = cyc[5];
+        ns.cycles_fold_row = cyc[6];
+        ns.cycles_fold_wait = cyc[7];
         ctx->nj_last = ns;
     }
-    if(err == 1) return set_error(ctx, MSA_ERR_DEVICE_TIMEOUT, "neighbor-joining grid barrier timed out");
     if(err == 2) return set_error(ctx, MSA_ERR_UNDEFINED, "no joinable pair: every Q value is NaN");
 
-    // star tree (src/phylogeny/njoining/star.cuh:61-72).
+    // star tree (src/phylogeny/njoining/star.cuh:61-72). The kernel records
+    // logical indices; the OTU in each slot follows the same window moves
+    // (slot of x gets the parent; logical 0's OTU moves into y's slot).
     const uint32_t nodes = 2 * n - 1;
     for(uint32_t k = 0; k < nodes; ++k) {
         out[k].parent = out[k].child[0] = out[k].child[1] = 0xffffffffu;
         out[k].distance = FLT_MAX;
         out[k].level = 0;
     }
+    std::vector<uint32_t> map(n);
+    for(uint32_t k = 0; k < n; ++k) map[k] = k;
     for(uint32_t k = 0; k + 1 < n; ++k) {
         const uint32_t parent = n + k;
-        const uint32_t a = rx[k], b = ry[k];
+        const uint32_t a = map[k + rx[k]], b = map[k + ry[k]];
+        map[k + rx[k]] = parent;
+        if(ry[k] != 0) map[k + ry[k]] = map[k];
         const uint32_t c1 = a < b ? a : b, c2 = a < b ? b : a;
         const float d1 = a < b ? rdx[k] : rdy[k], d2 = a < b ? rdy[k] : rdx[k];
         out[c1].distance = d1;

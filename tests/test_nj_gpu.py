@@ -32,14 +32,50 @@ def test_c1_tree_matches_reference(gpu, golden):
     assert_same_tree(phylogeny.run_triangle(tri.astype(np.float32), 16), golden["c1"]["tree"])
 
 
-@pytest.mark.parametrize("n,kind", [(2, "ties"), (3, "ties"), (4, "wide"), (17, "ties"), (200, "ties"),
-                                    (700, "wide"), (1100, "ties"), (1500, "wide")])
-def test_random_matrices_match_oracle(gpu, n, kind):
-    rng = np.random.default_rng(1000 + n)
+def _matrix(n, kind, rng):
     m = n * (n - 1) // 2
-    tri = {"ties": rng.integers(-3, 4, m), "wide": rng.integers(-5000, 5000, m)}[kind].astype(np.float32)
+    if kind == "ties":       # few distinct values: ties decide most joins
+        return rng.integers(-3, 4, m).astype(np.float32)
+    if kind == "wide":
+        return rng.integers(-5000, 5000, m).astype(np.float32)
+    if kind == "fraction":   # full 24-bit significands
+        return (rng.standard_normal(m) * 1000).astype(np.float32)
+    if kind == "tiny":       # subnormal distances: halved updates lose bits, so the
+        # new row sum takes the double-precision fold
+        return (rng.integers(1, 64, m) * np.float32(1.4e-45)).astype(np.float32)
+    raise ValueError(kind)
+
+
+# Odd sizes exercise row pitches padded to 4 floats; 2100 is larger than the
+# pipeline-scale workload.
+@pytest.mark.parametrize("n,kind", [(2, "ties"), (3, "ties"), (4, "wide"), (5, "ties"), (6, "wide"), (9, "ties"),
+                                    (17, "ties"), (33, "wide"), (130, "fraction"), (200, "ties"), (300, "tiny"),
+                                    (700, "wide"), (1100, "ties"), (1500, "wide"), (2100, "fraction")])
+def test_random_matrices_match_oracle(gpu, n, kind):
+    tri = _matrix(n, kind, np.random.default_rng(1000 + n))
     want = O.oracle_nj(tri, n)
     assert_same_tree(phylogeny.run_triangle(tri, n), want)
+
+
+def test_all_nan_matrix_is_an_error(gpu):
+    from msa_b200._lib import MsaError
+    tri = np.full(10 * 9 // 2, np.nan, np.float32)
+    with pytest.raises(MsaError):
+        phylogeny.run_triangle(tri, 10)
+    # the context stays usable
+    tri = _matrix(10, "wide", np.random.default_rng(7))
+    assert_same_tree(phylogeny.run_triangle(tri, 10), O.oracle_nj(tri, 10))
+
+
+def test_stats_report_the_cluster(gpu):
+    import ctypes
+    from msa_b200 import _lib, runtime
+    tri = _matrix(400, "wide", np.random.default_rng(8))
+    phylogeny.run_triangle(tri, 400)
+    ns = _lib.MsaNjStats()
+    _lib.check(_lib.lib().msa_nj_last_stats(runtime.context(0).handle, ctypes.byref(ns)))
+    assert ns.n == 400 and ns.cluster in (2, 4, 8, 16)
+    assert ns.kernel_ms > 0 and ns.cycles_fold > 0 and ns.cycles_scan > 0
 
 
 def test_c4_tree_matches_reference(gpu):
