@@ -48,12 +48,12 @@ namespace njdev {
 namespace cg = cooperative_groups;
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kThreads = 512;
+constexpr int kThreads = 1024;
 constexpr int kWarps = kThreads / 32;
 constexpr unsigned kMaxCluster = 16;
 constexpr uint32_t kNone = 0xffffffffu;
 // Row chunks (4 floats) each lane has in flight while scanning.
-constexpr int kBatch = 16;
+constexpr int kBatch = 4;
 // Phase counters: CTA 0 (scan, wait at A, join, wait at B, writes) and the
 // folding CTA (fold, scan of the new node's row, wait at A).
 constexpr int kCycleSlots = 8;
@@ -115,6 +115,8 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
     // Phase cycle counters live in shared memory, leaving registers to the
     // scan's loads in flight.
     __shared__ unsigned long long cyc[kCycleSlots];
+    // Row sum of `moved` while this CTA's S holds +inf in its slot (CTAs 0..F-1).
+    __shared__ float s_moved_sh;
 
     const unsigned K = cluster.num_blocks();
     const unsigned rank = cluster.block_rank();
@@ -124,6 +126,7 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
     float *D = st.D;
     const bool timer = tid == 0 && (rank == 0 || folder);
     if(tid < kCycleSlots) cyc[tid] = 0;
+    if(tid == 0) s_moved_sh = 0.0f;
     unsigned long long t_last = clock64();
     auto mark = [&](int k) {
         const unsigned long long now = clock64();
@@ -161,69 +164,88 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
         // ---- scan
         if(!folder) {
             // Rows i = 1..c-1 of the logical lower triangle; warp w takes rows
-            // w and 2W-1-w of every 2W, so a long and a short row pair up, and
-            // loads the pair's chunks kBatch at a time per lane.
+            // w and 2W-1-w of every 2W, so long and short rows pair up. This
+            // CTA's copy of S holds +inf in the dropped slots (< t) and in
+            // `moved`'s slot, so those columns give Q = -inf or NaN and never
+            // win; the new node's column and the cells past a row's end are
+            // masked. Each lane keeps, per row, the largest chunk maximum and
+            // the first chunk reaching it, and its best over rows by (Q, row,
+            // chunk), which orders like the row-major index; the element
+            // inside the winning chunk is resolved once, after the scan.
             const uint32_t W = F * kWarps;
             const uint32_t gw = rank * kWarps + warp;
             const uint32_t skip1 = pend == kNone ? kNone : t + pend;
-            const uint32_t skip2 = moved == kNone ? kNone : t + moved;
             const uint32_t base4 = t & ~3u;
-            const float s_moved = moved == kNone ? 0.0f : S[t + moved];
-            auto chunk = [&](const float4 &d, uint32_t col, uint32_t hi, float si, float &bq, uint32_t &bc) {
+            const float s_moved = s_moved_sh;
+            auto row_of = [&](uint32_t i) { return D + (size_t) (i == moved ? t - 1 : t + i) * P + base4; };
+            auto chunk_q = [&](const float4 &d, uint32_t col, uint32_t hi, float si, float &q0, float &q1, float &q2,
+                               float &q3) {
                 const float4 s = *reinterpret_cast<const float4 *>(S + col);
-                const float q0 = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d.x), si), s.x);
-                const float q1 = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d.y), si), s.y);
-                const float q2 = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d.z), si), s.z);
-                const float q3 = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d.w), si), s.w);
-                if(col >= t && col + 4 <= hi && skip1 - col >= 4u && skip2 - col >= 4u) {
-                    if(q0 > bq) { bq = q0; bc = col; }
-                    if(q1 > bq) { bq = q1; bc = col + 1; }
-                    if(q2 > bq) { bq = q2; bc = col + 2; }
-                    if(q3 > bq) { bq = q3; bc = col + 3; }
-                } else {
-                    auto ok = [&](uint32_t k) { return k >= t && k < hi && k != skip1 && k != skip2; };
-                    if(ok(col) && q0 > bq) { bq = q0; bc = col; }
-                    if(ok(col + 1) && q1 > bq) { bq = q1; bc = col + 1; }
-                    if(ok(col + 2) && q2 > bq) { bq = q2; bc = col + 2; }
-                    if(ok(col + 3) && q3 > bq) { bq = q3; bc = col + 3; }
+                q0 = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d.x), si), s.x);
+                q1 = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d.y), si), s.y);
+                q2 = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d.z), si), s.z);
+                q3 = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d.w), si), s.w);
+                if(col + 4 > hi || skip1 - col < 4u) {
+                    if(col >= hi || col == skip1) q0 = -INFINITY;
+                    if(col + 1 >= hi || col + 1 == skip1) q1 = -INFINITY;
+                    if(col + 2 >= hi || col + 2 == skip1) q2 = -INFINITY;
+                    if(col + 3 >= hi || col + 3 == skip1) q3 = -INFINITY;
                 }
             };
+            unsigned long long lbest = 0;   // (key << 32) | ~(row << 14 | chunk)
             for(uint32_t base = 0; base + 1 < c; base += 2 * W) {
-                uint32_t ia = base + 1 + gw, ib = base + 2 * W - gw;
-                if(ia >= c || ia == pend) ia = kNone;
-                if(ib >= c || ib == pend) ib = kNone;
-                const uint32_t na = ia == kNone ? 0 : (t + ia - base4 + 3) >> 2;
-                const uint32_t nb = ib == kNone ? 0 : (t + ib - base4 + 3) >> 2;
-                const float *rowa = D + (size_t) (ia == kNone ? t : ia == moved ? t - 1 : t + ia) * P + base4;
-                const float *rowb = D + (size_t) (ib == kNone ? t : ib == moved ? t - 1 : t + ib) * P + base4;
-                // Column `moved` of a later row: lane 0 for row a, lane 1 for row b.
-                const uint32_t ir = lane == 0 ? ia : ib;
-                const bool redirect = lane < 2 && moved != kNone && ir != kNone && ir > moved;
-                const float dm = redirect ? __ldcg(D + (size_t) (t + ir) * P + t - 1) : 0.0f;
-                const float sa = ia == kNone ? 0.0f : S[t + ia], sb = ib == kNone ? 0.0f : S[t + ib];
-                float bqa = -INFINITY, bqb = -INFINITY;
-                uint32_t bca = 0, bcb = 0;
-                for(uint32_t g0 = 0; g0 < na + nb; g0 += 32 * kBatch) {
-                    float4 d[kBatch];
+#pragma unroll 1
+                for(int h = 0; h < 2; ++h) {
+                    const uint32_t i = base + 1 + (h ? 2 * W - 1 - gw : gw);
+                    if(i >= c || i == pend) continue;
+                    const uint32_t hi = t + i;
+                    const float *row = row_of(i);
+                    const float si = i == moved ? s_moved : S[t + i];
+                    const uint32_t nch = (hi - base4 + 3) >> 2;
+                    float bq = -INFINITY;
+                    uint32_t bg = 0;
+                    for(uint32_t g0 = lane; g0 < nch; g0 += 32 * kBatch) {
+                        float4 d[kBatch];
 #pragma unroll
-                    for(int u = 0; u < kBatch; ++u) {
-                        const uint32_t g = g0 + lane + 32 * u;
-                        if(g < na) d[u] = __ldcg(reinterpret_cast<const float4 *>(rowa + 4 * g));
-                        else if(g < na + nb) d[u] = __ldcg(reinterpret_cast<const float4 *>(rowb + 4 * (g - na)));
+                        for(int u = 0; u < kBatch; ++u)
+                            if(g0 + 32 * u < nch) d[u] = __ldcg(reinterpret_cast<const float4 *>(row + 4 * (g0 + 32 * u)));
+#pragma unroll
+                        for(int u = 0; u < kBatch; ++u) {
+                            const uint32_t g = g0 + 32 * u;
+                            if(g < nch) {
+                                float q0, q1, q2, q3;
+                                chunk_q(d[u], base4 + 4 * g, hi, si, q0, q1, q2, q3);
+                                const float m = fmaxf(fmaxf(q0, q1), fmaxf(q2, q3));
+                                if(m > bq) {
+                                    bq = m;
+                                    bg = g;
+                                }
+                            }
+                        }
                     }
-#pragma unroll
-                    for(int u = 0; u < kBatch; ++u) {
-                        const uint32_t g = g0 + lane + 32 * u;
-                        if(g < na) chunk(d[u], base4 + 4 * g, t + ia, sa, bqa, bca);
-                        else if(g < na + nb) chunk(d[u], base4 + 4 * (g - na), t + ib, sb, bqb, bcb);
+                    const uint32_t key = order_key(bq);
+                    if(key) lbest = umax64(lbest, ((unsigned long long) key << 32) | (0xffffffffu - ((i << 14) | bg)));
+                    // Column `moved` of a later row, from where logical 0's data still is.
+                    if(lane == 0 && moved != kNone && i > moved) {
+                        const float dm = __ldcg(D + (size_t) (t + i) * P + t - 1);
+                        const float q = __fsub_rn(__fsub_rn(__fmul_rn(cm2, dm), si), s_moved);
+                        offer(pack(order_key(q), i * (i - 1) / 2 + moved), i, moved);
                     }
                 }
-                if(ia != kNone && order_key(bqa)) offer(pack(order_key(bqa), ia * (ia - 1) / 2 + (bca - t)), ia, bca - t);
-                if(ib != kNone && order_key(bqb)) offer(pack(order_key(bqb), ib * (ib - 1) / 2 + (bcb - t)), ib, bcb - t);
-                if(redirect) {
-                    const float q = __fsub_rn(__fsub_rn(__fmul_rn(cm2, dm), lane == 0 ? sa : sb), s_moved);
-                    offer(pack(order_key(q), ir * (ir - 1) / 2 + moved), ir, moved);
-                }
+            }
+            if(lbest) {
+                const uint32_t tail = 0xffffffffu - (uint32_t) (lbest & 0xffffffffull);
+                const uint32_t i = tail >> 14, g = tail & 0x3fffu, col = base4 + 4 * g;
+                const float si = i == moved ? s_moved : S[t + i];
+                float q[4];
+                chunk_q(__ldcg(reinterpret_cast<const float4 *>(row_of(i) + 4 * g)), col, t + i, si, q[0], q[1], q[2], q[3]);
+                const uint32_t key = (uint32_t) (lbest >> 32);
+                int k = 3;
+                if(order_key(q[2]) == key) k = 2;   // keep the first element equal to the maximum
+                if(order_key(q[1]) == key) k = 1;
+                if(order_key(q[0]) == key) k = 0;
+                const uint32_t j = col + k - t;
+                offer(pack(key, i * (i - 1) / 2 + j), i, j);
             }
         } else if(pend != kNone) {
             // The new node's row and column, from the distances the last join
@@ -292,6 +314,9 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
         const uint32_t wi = wlo + tid;
         const float v0 = (wi < whi && y != 0) ? __ldcg(r0 + wi) : 0.0f;
 
+        // The scan is over: `moved`'s row sum goes back into its slot.
+        if(!folder && tid == 0 && moved != kNone) S[t + moved] = s_moved_sh;
+
         // raise_candidate (sequential.cpp:142-152) and the join record.
         if(rank == 0 && tid == 0) {
             const float pairsum = __fsub_rn(S[t + x], S[t + y]);
@@ -334,7 +359,19 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
         }
         exact = __syncthreads_and(exact);
         // update_cache (sequential.cpp:210-224): logical 0 takes y's place.
-        if(y != 0 && tid == 0) S[t + y] = S[t];
+        // The scanning CTAs keep that row sum aside and put +inf in its slot
+        // and in logical 0's (dropped next) for the next scan.
+        if(tid == 0) {
+            if(folder) {
+                if(y != 0) S[t + y] = S[t];
+            } else {
+                if(y != 0) {
+                    s_moved_sh = S[t];
+                    S[t + y] = INFINITY;
+                }
+                S[t] = INFINITY;
+            }
+        }
         if(timer && rank == 0) mark(2);
         cluster_arrive();   // B: every read of rows x, y and 0 is done
         cluster_wait();
