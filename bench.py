@@ -162,6 +162,72 @@ def reference_arm(args):
     print(json.dumps(line))
 
 
+# ---------------------------------------------------------------- NJ leg
+
+def nj_algorithmic_bytes(n: int) -> int:
+    """Bytes one NJ run must move at the least: each join with c OTUs reads the
+    c(c-1)/2 lower-triangle distances and the c row sums, reads rows x and y
+    and writes row and column x and the copy of logical 0 into y (6c floats)."""
+    return sum(4 * (c * (c - 1) // 2 + c + 6 * c) for c in range(2, n + 1))
+
+
+def nj_leg(lib, ctx, steps: int = 3, cpu: bool = True) -> dict:
+    """Neighbor-joining of the 2000-taxon pipeline workload: the NW scores stay
+    on the device and feed msa_nj directly (int32 triangle). Reports the NJ
+    kernel time, algorithmic bytes per second, and the reference's sequential
+    NJ on the host for the same matrix (with a topology check)."""
+    import ctypes
+
+    import torch
+
+    from msa_b200 import ScoringTable, _lib
+    wl = load_workload("c4")
+    n = wl.n
+    flat, offs, lens = wl.flat_units()
+    u8, u64 = ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint64)
+    h = ctypes.c_uint64()
+    _lib.check(lib.msa_seqs_upload(ctx.handle, flat.ctypes.data_as(u8), offs.ctypes.data_as(u64),
+                                   lens.ctypes.data_as(u64), n, ctypes.byref(h)), ctx.handle)
+    tri = torch.empty(n * (n - 1) // 2, dtype=torch.int32, device=torch.cuda.current_device())
+    table = ScoringTable(wl.table)
+    _lib.check(lib.msa_nw_all_pairs(ctx.handle, h.value, ctypes.byref(table._t), _lib.MSA_NW_PERSISTENT,
+                                    ctypes.c_void_p(tri.data_ptr()), 1), ctx.handle)
+    lib.msa_seqs_release(ctx.handle, h.value)
+    nodes = (_lib.MsaOtu * (2 * n - 1))()
+    kms, tms = [], []
+    for s in range(1 + steps):
+        _lib.check(lib.msa_nj(ctx.handle, ctypes.c_void_p(tri.data_ptr()), _lib.MSA_TRI_I32_DEVICE, n, nodes),
+                   ctx.handle)
+        st = _lib.MsaNjStats()
+        lib.msa_nj_last_stats(ctx.handle, ctypes.byref(st))
+        if s >= 1:
+            kms.append(st.kernel_ms)
+            tms.append(st.total_ms)
+    kernel_ms = float(np.mean(kms))
+    alg = nj_algorithmic_bytes(n)
+    out = {"workload": "2000 proteins, 20 clades of 100 (c4 scores, int32 on the device)", "otus": n,
+           "joins": n - 1, "kernel_ms": kernel_ms, "total_ms": float(np.mean(tms)), "steps": steps,
+           "us_per_join": 1e3 * kernel_ms / (n - 1), "algorithmic_bytes": alg,
+           "achieved_GBps": alg / (kernel_ms / 1e3) / 1e9, "cluster_ctas": int(st.cluster),
+           "note": "the 16 MB distance matrix stays in L2 (126 MB); the bound is per-join latency"}
+    if cpu:
+        from oracle import oracle as O
+        if O.reference() is not None:
+            host = tri.cpu().numpy()
+            t0 = time.perf_counter()
+            ref = O.ref_nj(host.astype(np.float32), n)
+            ref_ms = (time.perf_counter() - t0) * 1e3
+            arr = np.frombuffer(nodes, dtype=np.dtype([("parent", "<u4"), ("c0", "<u4"), ("c1", "<u4"),
+                                                       ("distance", "<f4"), ("level", "<u4")]))
+            out["cpu_reference"] = {"ms": ref_ms, "cores": 1, "kind": "reference",
+                                    "sample": "Museqa njoining::sequential (symmetric), oracle/_ref, full run"}
+            out["tree_matches_reference"] = bool(
+                (arr["parent"] == ref["parent"]).all() and (arr["c0"] == ref["child0"]).all()
+                and (arr["c1"] == ref["child1"]).all()
+                and (arr["distance"].view(np.uint32) == np.asarray(ref["distance"], np.float32).view(np.uint32)).all())
+    return out
+
+
 # ---------------------------------------------------------------- GPU arm
 
 PROBE_OPS = ["iadd", "imnmx", "viaddmax_s32", "vimax3_s32", "vadd2", "viaddmax_s16x2", "vimax3_s16x2",
@@ -307,6 +373,7 @@ def main():
     ap.add_argument("--plain-steps", type=int, default=1)
     ap.add_argument("--cpu-cells", type=float, default=1.5e10)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-nj", action="store_true", help="skip the neighbor-joining leg")
     ap.add_argument("--profile", choices=["persistent", "plain", "nj"], default=None,
                     help="profiling run: --warmup calls then one call, on the first --n sequences")
     ap.add_argument("--n", type=int, default=0, help="with --profile: use the first N sequences")
@@ -475,6 +542,8 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
+        if not args.no_nj:
+            line["nj"] = nj_leg(lib, ctx, cpu=not args.no_cpu)
         print(json.dumps(line))
     if world > 1:
         dist.barrier()

@@ -306,7 +306,10 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
         const float *rx = D + (size_t) (t + x) * P + t;
         const float *ry = D + (size_t) (t + y) * P + t;
         const float *r0 = D + (size_t) t * P + t;
+        // Every load this thread's first join element needs is issued here,
+        // before the bookkeeping below: one L2 round trip for all of them.
         const float dxy = __ldcg(rx + y);
+        float a = (uint32_t) tid < c ? __ldcg(rx + tid) : 0.0f, b = (uint32_t) tid < c ? __ldcg(ry + tid) : 0.0f;
         // This thread's first element of the write slice (CTAs 0..F-1):
         // logical 0's entry, loaded now so the writes wait for no load.
         const uint32_t wlo = folder ? 0 : (uint32_t) ((uint64_t) c * rank / F);
@@ -341,9 +344,7 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
         // i = y read the diagonal and D[x][y], as the reference does.
         bool exact = true;
         {
-            uint32_t i = tid;
-            float a = i < c ? __ldcg(rx + i) : 0.0f, b = i < c ? __ldcg(ry + i) : 0.0f;
-            for(; i < c; i += kThreads) {
+            for(uint32_t i = tid; i < c; i += kThreads) {
                 const uint32_t in = i + kThreads;
                 const float an = in < c ? __ldcg(rx + in) : 0.0f, bn = in < c ? __ldcg(ry + in) : 0.0f;
                 const float prev = __fadd_rn(a, b);
@@ -380,14 +381,14 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             // Serial fold of the new row sum, i ascending. When every update is
             // a float value, the double add rounded to float equals a float add
             // (double has >= 2*24+2 significand bits), so the short float chain
-            // is used; otherwise the literal double one. Warp 0 runs it: each
-            // chunk of 32 updates is loaded one per lane (the next chunk while
-            // the current one is added) and handed out by shuffles, and every
-            // lane adds the same chain, so no lane diverges.
+            // is used; otherwise the literal double one. Warp 0 runs it.
             if(warp == 0) {
                 const unsigned long long f0 = clock64();
                 float ns = 0.0f;
                 if(exact) {
+                    // Each chunk of 32 updates is loaded one per lane (the next
+                    // chunk while this one is added) and handed out by
+                    // shuffles; every lane adds the same chain.
                     float v = (uint32_t) lane < c ? ND[lane] : 0.0f;
                     for(uint32_t base = 0; base < c; base += 32) {
                         const float cur = v;
