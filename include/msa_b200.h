@@ -147,6 +147,28 @@ typedef enum msa_nw_mode {
 int msa_nw_all_pairs(msa_ctx *ctx, msa_seqs seqs, const msa_table *table, int mode,
                      int32_t *out, int out_on_device);
 
+/*
+ * One part of an all-pairs job split over several devices. Replaces the
+ * reference's MPI split of the pair list over ranks
+ * (src/pairwise/needleman/needleman.cpp:31-52, utils::partition at
+ * src/utils.hpp:176-183), which gives every rank the same number of pairs;
+ * here the parts hold about equal DP cells. Scores exactly the pairs that
+ * msa_nw_part_of_pairs assigns to `part` (0 <= part < nparts) and writes
+ * only their entries of `out` (n(n-1)/2 int32 at i(i-1)/2+j); every other
+ * entry keeps its value. Scores equal msa_nw_all_pairs's. Every device given
+ * the same sequences, table, mode and nparts computes the same split, so
+ * zero-filled outputs of all parts summed (or the parts written into one
+ * buffer) give the whole matrix.
+ */
+int msa_nw_all_pairs_part(msa_ctx *ctx, msa_seqs seqs, const msa_table *table, int mode, uint32_t part,
+                          uint32_t nparts, int32_t *out, int out_on_device);
+
+/* Host-only: the part (0..nparts-1) that msa_nw_all_pairs_part assigns to
+ * every pair, written at i(i-1)/2+j of `out_part` (n(n-1)/2 entries). Needs
+ * no device. */
+int msa_nw_part_of_pairs(const uint8_t *units, const uint64_t *offs, const uint64_t *lens, uint32_t n,
+                         const msa_table *table, uint32_t nparts, uint32_t *out_part);
+
 /* Tile shape of the persistent kernel: rows per lane (16 or 32) and warps per
  * CTA (4 or 8); 0, 0 restores the committed autotuned choice. No counterpart
  * in the reference (its one kernel shape is fixed, hybrid.cu:57). */

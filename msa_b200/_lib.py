@@ -114,6 +114,11 @@ _PROTOS = [
     ("msa_seqs_count", ctypes.c_int64, [ctypes.c_void_p, ctypes.c_uint64]),
     ("msa_nw_all_pairs", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(MsaTable), ctypes.c_int,
                                         ctypes.c_void_p, ctypes.c_int]),
+    ("msa_nw_all_pairs_part", ctypes.c_int, [ctypes.c_void_p, ctypes.c_uint64, ctypes.POINTER(MsaTable), ctypes.c_int,
+                                             ctypes.c_uint32, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_int]),
+    ("msa_nw_part_of_pairs", ctypes.c_int, [ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint64),
+                                            ctypes.POINTER(ctypes.c_uint64), ctypes.c_uint32, ctypes.POINTER(MsaTable),
+                                            ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]),
     ("msa_nw_set_tiles", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
     ("msa_nw_all_pairs_noalloc", ctypes.c_int, [ctypes.c_void_p, c_u64p, c_u64p, ctypes.c_uint32,
                                                 ctypes.POINTER(MsaTable), ctypes.c_void_p, ctypes.c_void_p]),

@@ -17,7 +17,11 @@ LIB = PKG / "libmsa_b200.so"
 BUILD_DIR = PKG / "_build"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-SOURCES = ["tables.cpp", "abi.cpp", "nw_kernels.cu", "nj_kernel.cu", "probe.cu", "noalloc.cu", "serve.cpp"]
+SOURCES = ["tables.cpp", "abi.cpp", "partition.cpp", "nw_kernels.cu", "nj_kernel.cu", "probe.cu", "noalloc.cu",
+           "serve.cpp", "facade.cu"]
+# The command line (museqa), linked against the library.
+CLI = PKG / "museqa"
+CLI_SOURCE = "cli.cpp"
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-O3",
               "--expt-relaxed-constexpr", "-I", str(INCLUDE)]
 
@@ -29,11 +33,11 @@ def _nvcc() -> str:
 
 
 def _stale() -> bool:
-    if not LIB.exists():
+    if not LIB.exists() or not CLI.exists():
         return True
-    t = LIB.stat().st_mtime
-    deps = [CSRC / s for s in SOURCES] + list(CSRC.glob("*.hpp")) + list(CSRC.glob("*.cuh")) \
-        + list(CSRC.glob("*.inc")) + list(INCLUDE.glob("*.h")) + [Path(__file__)]
+    t = min(LIB.stat().st_mtime, CLI.stat().st_mtime)
+    deps = [CSRC / s for s in SOURCES] + [CSRC / CLI_SOURCE] + list(CSRC.glob("*.hpp")) + list(CSRC.glob("*.cuh")) \
+        + list(CSRC.glob("*.inc")) + list(INCLUDE.glob("*.h")) + list(INCLUDE.glob("*.hpp")) + [Path(__file__)]
     return any(p.exists() and p.stat().st_mtime > t for p in deps)
 
 
@@ -57,6 +61,13 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         print(" ".join(cmd), flush=True)
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
+    cli_tmp = CLI.with_suffix(".tmp")
+    cmd = [nvcc, *ARCH, *NVCC_FLAGS, "-x", "cu", str(CSRC / CLI_SOURCE), "-o", str(cli_tmp), "-L", str(PKG),
+           "-lmsa_b200", "-Xlinker", "-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.run(cmd, check=True)
+    os.replace(cli_tmp, CLI)
     return LIB
 
 

@@ -163,29 +163,16 @@ int build_store(msa_ctx *ctx, const uint8_t *units, const uint64_t *offs, const 
         for(uint32_t i = 0; i < n; ++i) {
             const uint8_t *src = units + offs[i];
             uint8_t *dst = host.data() + st->off[i];
-            uint32_t first_end = st->plen[i];
-            bool seen_end = false, dirty = false, gap = false;
             for(uint64_t k = 0; k < st->len[i]; ++k) {
                 const uint8_t u = src[k];
                 if(u > MSA_UNIT_GAP) { free_store(st); return set_error(ctx, MSA_ERR_INVALID, "unit code above 25"); }
                 dst[k] = u;
-                if(u == MSA_UNIT_END) {
-                    if(!seen_end) { first_end = (uint32_t) k; seen_end = true; }
-                } else if(seen_end) {
-                    dirty = true;
-                }
-                if(u == MSA_UNIT_GAP) gap = true;
             }
-            if(!seen_end && st->len[i] < st->plen[i]) first_end = (uint32_t) st->len[i];
-            st->eff[i] = first_end;
-            st->has_gap[i] = gap;
-            st->dirty[i] = (dirty || first_end == 0 || gap) ? 1 : 0;
-            st->any_gap |= gap;
+            scan_units(src, st->len[i], st->plen[i], &st->eff[i], &st->dirty[i], &st->has_gap[i]);
+            st->any_gap |= st->has_gap[i] != 0;
         }
         // Clean sequences sorted by effective length, longest first.
-        for(uint32_t i = 0; i < n; ++i) if(!st->dirty[i]) st->clean_sorted.push_back(i);
-        std::stable_sort(st->clean_sorted.begin(), st->clean_sorted.end(),
-                         [st](uint32_t a, uint32_t b) { return st->eff[a] > st->eff[b]; });
+        sort_clean(st->eff, st->dirty, st->clean_sorted);
         // Profile geometry.
         st->prof_off.resize(n);
         st->prof_lp.resize(n);
@@ -275,10 +262,22 @@ int64_t msa_seqs_count(msa_ctx *ctx, msa_seqs seqs)
     return it == ctx->stores.end() ? -1 : (int64_t) it->second->n;
 }
 
-int msa_nw_all_pairs(msa_ctx *ctx, msa_seqs seqs, const msa_table *table, int mode, int32_t *out,
-                     int out_on_device)
+}  // extern "C"
+
+namespace msa {
+
+bool table_is_symmetric(const ExtTable &t)
 {
-    if(!ctx || !table) return MSA_ERR_INVALID;
+    for(int x = 0; x < 25; ++x)
+        for(int y = 0; y < 25; ++y)
+            if(t.score[x * kAlpha + y] != t.score[y * kAlpha + x]) return false;
+    return true;
+}
+
+static int all_pairs(msa_ctx *ctx, msa_seqs seqs, const msa_table *table, int mode, uint32_t part, uint32_t nparts,
+                     int32_t *out, int out_on_device)
+{
+    if(!ctx || !table || nparts == 0 || part >= nparts) return MSA_ERR_INVALID;
     try {
         auto it = ctx->stores.find(seqs);
         if(it == ctx->stores.end()) return set_error(ctx, MSA_ERR_HANDLE, "unknown sequence store");
@@ -308,10 +307,7 @@ int msa_nw_all_pairs(msa_ctx *ctx, msa_seqs seqs, const msa_table *table, int mo
         if(vb >= (1ll << 30)) return set_error(ctx, MSA_ERR_TOO_LARGE, "scores could exceed the int32 range");
         // Tables that are not symmetric make the score depend on orientation:
         // route every pair through the reference-orientation path.
-        bool symmetric = true;
-        for(int x = 0; x < 25 && symmetric; ++x)
-            for(int y = 0; y < 25; ++y)
-                if(ext.score[x * kAlpha + y] != ext.score[y * kAlpha + x]) { symmetric = false; break; }
+        const bool symmetric = table_is_symmetric(ext);
         std::vector<uint8_t> saved_dirty;
         std::vector<uint32_t> saved_sorted;
         if(!symmetric) {
@@ -328,16 +324,41 @@ int msa_nw_all_pairs(msa_ctx *ctx, msa_seqs seqs, const msa_table *table, int mo
             d_out = (int32_t *) ctx->out_tmp.ptr;
         }
         if(npairs && !out) return MSA_ERR_INVALID;
-        rc = nw_run(ctx, st, ext, mode, d_out);
+        rc = nw_run(ctx, st, ext, mode, d_out, part, nparts);
+        std::vector<uint32_t> owner;
+        if(!out_on_device && npairs && nparts > 1 && !rc) {
+            // Host output of one part: only that part's entries are written.
+            owner.resize(npairs);
+            std::vector<uint32_t> gpairs;
+            list_generic_pairs(st->dirty, st->len, gpairs);
+            const JobSplit s = split_job(st->eff, st->plen, st->clean_sorted, gpairs, nparts);
+            std::fill(owner.begin(), owner.end(), nparts);
+            auto tri = [](uint64_t i, uint64_t j) { return i > j ? i * (i - 1) / 2 + j : j * (j - 1) / 2 + i; };
+            const auto &cs = st->clean_sorted;
+            for(uint32_t k = s.k[part]; k < s.k[part + 1]; ++k)
+                for(uint32_t a = 2 * k; a < std::min<uint32_t>(2 * k + 2, (uint32_t) cs.size()); ++a)
+                    for(uint32_t b = a + 1; b < (uint32_t) cs.size(); ++b) owner[tri(cs[a], cs[b])] = part;
+            for(uint64_t q = s.g[part]; q < s.g[part + 1]; ++q) owner[tri(gpairs[2 * q], gpairs[2 * q + 1])] = part;
+        }
         if(!symmetric) {
             st->dirty = saved_dirty;
             st->clean_sorted = saved_sorted;
         }
         if(rc) return rc;
         if(!out_on_device && npairs) {
-            cudaError_t e = cudaMemcpyAsync(out, d_out, npairs * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
-            if(!e) e = cudaStreamSynchronize(ctx->stream);
-            if(e) return cuda_error(ctx, e, "copy scores to host");
+            if(nparts == 1) {
+                cudaError_t e = cudaMemcpyAsync(out, d_out, npairs * sizeof(int32_t), cudaMemcpyDeviceToHost, ctx->stream);
+                if(!e) e = cudaStreamSynchronize(ctx->stream);
+                if(e) return cuda_error(ctx, e, "copy scores to host");
+            } else {
+                std::vector<int32_t> all(npairs);
+                cudaError_t e = cudaMemcpyAsync(all.data(), d_out, npairs * sizeof(int32_t), cudaMemcpyDeviceToHost,
+                                                ctx->stream);
+                if(!e) e = cudaStreamSynchronize(ctx->stream);
+                if(e) return cuda_error(ctx, e, "copy scores to host");
+                for(uint64_t q = 0; q < npairs; ++q)
+                    if(owner[q] == part) out[q] = all[q];
+            }
         }
         return MSA_OK;
     } catch(const std::bad_alloc &) {
@@ -345,6 +366,22 @@ int msa_nw_all_pairs(msa_ctx *ctx, msa_seqs seqs, const msa_table *table, int mo
     } catch(...) {
         return set_error(ctx, MSA_ERR_CUDA, "unexpected failure in msa_nw_all_pairs");
     }
+}
+
+}  // namespace msa
+
+extern "C" {
+
+int msa_nw_all_pairs(msa_ctx *ctx, msa_seqs seqs, const msa_table *table, int mode, int32_t *out,
+                     int out_on_device)
+{
+    return msa::all_pairs(ctx, seqs, table, mode, 0, 1, out, out_on_device);
+}
+
+int msa_nw_all_pairs_part(msa_ctx *ctx, msa_seqs seqs, const msa_table *table, int mode, uint32_t part,
+                          uint32_t nparts, int32_t *out, int out_on_device)
+{
+    return msa::all_pairs(ctx, seqs, table, mode, part, nparts, out, out_on_device);
 }
 
 int msa_nw_set_tiles(msa_ctx *ctx, int rows_per_lane, int warps_per_cta)

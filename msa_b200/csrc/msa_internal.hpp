@@ -106,7 +106,32 @@ namespace msa {
 
 // Kernel launchers (nw_kernels.cu). All launch on ctx->stream and count launches.
 struct NwPlan;
-int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d_out);
+// Scores the pairs of part `part` of `nparts` (split_job) into d_out; the
+// other entries of d_out are not written. part 0 of 1 is the whole job.
+int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d_out, uint32_t part = 0,
+           uint32_t nparts = 1);
+
+// Host-side sequence scan (the rules of a store upload): index of the first
+// END unit within the padded length, "dirty" (END units not forming a
+// suffix, empty, or a GAP unit) and GAP presence.
+void scan_units(const uint8_t *src, uint64_t len, uint32_t plen, uint32_t *eff, uint8_t *dirty, uint8_t *gap);
+// Clean sequences sorted by eff descending (ties: index ascending).
+void sort_clean(const std::vector<uint32_t> &eff, const std::vector<uint8_t> &dirty, std::vector<uint32_t> &out);
+// Pairs with at least one dirty sequence, row-major, each as (rows, columns)
+// in the reference's orientation.
+void list_generic_pairs(const std::vector<uint8_t> &dirty, const std::vector<uint64_t> &len,
+                        std::vector<uint32_t> &gpairs);
+// A job cut into parts of about equal DP cells: rows pairs [k[p], k[p+1]) of
+// the clean sorted order and generic pairs [g[p], g[p+1]).
+struct JobSplit {
+    std::vector<uint32_t> k;
+    std::vector<uint64_t> g;
+    std::vector<unsigned __int128> clean_cells;   // cumulative cells of rows pairs
+};
+JobSplit split_job(const std::vector<uint32_t> &eff, const std::vector<uint32_t> &plen,
+                   const std::vector<uint32_t> &clean_sorted, const std::vector<uint32_t> &gpairs, uint32_t parts);
+bool table_is_symmetric(const ExtTable &t);
+
 // Bytes of padding before the first sequence in a store's unit buffer.
 constexpr int kUnitFront = 64;
 int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out);

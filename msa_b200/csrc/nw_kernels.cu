@@ -386,7 +386,8 @@ struct BatchParams {
     JobView job;
     uint32_t npairs_rows;       // number of rows pairs, ceil(nclean / 2)
     const uint64_t *row_task;   // first task of each rows pair (npairs_rows + 1)
-    uint64_t ntasks;
+    uint64_t ntasks;            // tasks of this launch: task_base .. task_base + ntasks - 1
+    uint64_t task_base;
     uint32_t *bound;
     uint64_t bound_stride;
     unsigned long long *counter;
@@ -666,8 +667,8 @@ __global__ void __launch_bounds__(W * 32, BatchOcc<RMAX, W>::value) nw_batched_k
         __syncthreads();
         if(threadIdx.x == 0) task_q = atomicAdd(p.counter, 1ull);
         __syncthreads();
-        const unsigned long long q = task_q;
-        if(q >= p.ntasks) break;
+        if(task_q >= p.ntasks) break;
+        const unsigned long long q = task_q + p.task_base;
         uint32_t lo = 0, hi = p.npairs_rows - 1;
         while(lo < hi) {
             const uint32_t mid = (lo + hi + 1) >> 1;
@@ -898,6 +899,7 @@ struct NwPlan {
     uint64_t batch_grid = 0;
     uint32_t launches = 0, narrow_tasks = 0;
     uint64_t cells = 0, pairs = 0;
+    uint32_t part = 0, nparts = 1;
     cudaGraphExec_t exec = nullptr;
     cudaStream_t captured_on = nullptr;
     ~NwPlan()
@@ -952,7 +954,7 @@ static void launch_batched(const NwPlan &pl, cudaStream_t s)
 }
 
 static int build_plan(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d_out, Tiles tiles,
-                      NwPlan *pl)
+                      uint32_t part, uint32_t nparts, NwPlan *pl)
 {
     const uint32_t n = st->n;
     pl->store_serial = st->serial;
@@ -961,33 +963,38 @@ static int build_plan(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode,
     pl->tiles = tiles;
     pl->tbl = tbl;
     pl->n = n;
-    pl->pairs = (uint64_t) n * (n - 1) / 2;
-    // sum over pairs of L_i * L_j = ((sum L)^2 - sum L^2) / 2, in 128-bit arithmetic.
-    unsigned __int128 s1 = 0, s2 = 0;
-    for(uint32_t i = 0; i < n; ++i) { s1 += st->len[i]; s2 += (unsigned __int128) st->len[i] * st->len[i]; }
-    pl->cells = (uint64_t) ((s1 * s1 - s2) / 2);
+    pl->part = part;
+    pl->nparts = nparts;
 
     const uint32_t nclean = (uint32_t) st->clean_sorted.size();
     const uint64_t nclean_pairs = (uint64_t) nclean * (nclean > 0 ? nclean - 1 : 0) / 2;
 
-    // Pairs with at least one dirty sequence, in the reference's orientation.
-    std::vector<uint32_t> gpairs;
-    {
-        std::vector<uint8_t> isd(n, 0);
-        bool any = false;
-        for(uint32_t i = 0; i < n; ++i) if(st->dirty[i]) { isd[i] = 1; any = true; }
-        if(any) {
-            for(uint32_t i = 1; i < n; ++i) {
-                for(uint32_t j = 0; j < i; ++j) {
-                    if(!isd[i] && !isd[j]) continue;
-                    const uint64_t bi = (st->len[i] + 2) / 3, bj = (st->len[j] + 2) / 3;
-                    gpairs.push_back(bi > bj ? i : j);
-                    gpairs.push_back(bi > bj ? j : i);
-                }
-            }
-        }
-    }
+    // Pairs with at least one dirty sequence, in the reference's orientation,
+    // and this part's runs of rows pairs and generic pairs.
+    std::vector<uint32_t> gpairs_all;
+    list_generic_pairs(st->dirty, st->len, gpairs_all);
+    const JobSplit split = split_job(st->eff, st->plen, st->clean_sorted, gpairs_all, nparts);
+    const uint32_t k_lo = split.k[part], k_hi = split.k[part + 1];
+    const uint64_t g_lo = split.g[part], g_hi = split.g[part + 1];
+    const std::vector<uint32_t> gpairs(gpairs_all.begin() + 2 * g_lo, gpairs_all.begin() + 2 * g_hi);
     pl->ngeneric = gpairs.size() / 2;
+
+    // Pairs and cells (given lengths) of this part.
+    {
+        using u128 = unsigned __int128;
+        const auto &cs = st->clean_sorted;
+        std::vector<u128> suffix(nclean + 1, 0);
+        for(uint32_t b = nclean; b-- > 0;) suffix[b] = suffix[b + 1] + st->len[cs[b]];
+        u128 cells = 0;
+        uint64_t pairs = 0;
+        for(uint32_t a = 2 * k_lo; a < std::min<uint32_t>(2 * k_hi, nclean); ++a) {
+            cells += (u128) st->len[cs[a]] * suffix[a + 1];
+            pairs += nclean - 1 - a;
+        }
+        for(uint64_t q = 0; q < pl->ngeneric; ++q) cells += (u128) st->len[gpairs[2 * q]] * st->len[gpairs[2 * q + 1]];
+        pl->cells = (uint64_t) cells;
+        pl->pairs = pairs + pl->ngeneric;
+    }
 
     uint32_t max_cols = 1;
     for(uint32_t i = 0; i < n; ++i) max_cols = std::max(max_cols, st->plen[i]);
@@ -1007,6 +1014,7 @@ static int build_plan(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode,
     std::vector<uint8_t> row_narrow;
     uint64_t ntasks = 0;
     uint32_t K = 0;
+    uint64_t task_base = 0;
     if(mode == MSA_NW_PERSISTENT && nclean_pairs > 0) {
         const int SH = 32 * tiles.R;
         K = (nclean + 1) / 2;
@@ -1021,10 +1029,13 @@ static int build_plan(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode,
             const bool nar = narrow_ok(rows_p, cols, tbl);
             row_narrow[k] = nar ? 1 : 0;
             const uint64_t groups = (uint64_t) (ncol + tiles.W - 1) / tiles.W;
-            if(nar) pl->narrow_tasks += (uint32_t) groups;
+            if(nar && k >= k_lo && k < k_hi) pl->narrow_tasks += (uint32_t) groups;
             ntasks += groups;
         }
         row_task[K] = ntasks;
+        // This part's tasks: those of rows pairs [k_lo, k_hi).
+        task_base = row_task[k_lo];
+        ntasks = row_task[k_hi] - task_base;
         int rc;
         if(tiles.R == 16 && tiles.W == 4) rc = batched_grid<16, 4>(ctx, ntasks, &pl->batch_grid);
         else if(tiles.R == 16 && tiles.W == 8) rc = batched_grid<16, 8>(ctx, ntasks, &pl->batch_grid);
@@ -1087,6 +1098,7 @@ static int build_plan(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode,
     bp.npairs_rows = K;
     bp.row_task = (const uint64_t *) (base + o_rt);
     bp.ntasks = ntasks;
+    bp.task_base = task_base;
     bp.bound = p.bound;
     bp.bound_stride = stride;
     bp.counter = (unsigned long long *) (base + o_cnt);
@@ -1095,11 +1107,13 @@ static int build_plan(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode,
     if(mode == MSA_NW_PLAIN && nclean_pairs > 0) {
         // Buckets: runs of sorted rows with the same strip count.
         constexpr int SH = 32 * kPlainR;
-        uint32_t a = 0;
-        while(a + 1 < nclean) {
+        // This part's rows: sorted [2 k_lo, 2 k_hi).
+        const uint32_t a_end = std::min<uint32_t>(2 * k_hi, nclean);
+        uint32_t a = std::min<uint32_t>(2 * k_lo, nclean);
+        while(a < a_end && a + 1 < nclean) {
             const uint32_t strips = (st->eff[st->clean_sorted[a]] + SH - 1) / SH;
             uint32_t a2 = a + 1;
-            while(a2 + 1 < nclean && (st->eff[st->clean_sorted[a2]] + SH - 1) / SH == strips) ++a2;
+            while(a2 < a_end && a2 + 1 < nclean && (st->eff[st->clean_sorted[a2]] + SH - 1) / SH == strips) ++a2;
             const uint64_t k_lo = (uint64_t) a * (2 * (uint64_t) nclean - a - 1) / 2;
             const uint64_t k_hi = (uint64_t) a2 * (2 * (uint64_t) nclean - a2 - 1) / 2;
             pl->plain.push_back({k_lo, k_hi, std::min<uint64_t>(resident_blocks, (k_hi - k_lo + kWPB - 1) / kWPB)});
@@ -1151,7 +1165,8 @@ static bool same_table(const ExtTable &a, const ExtTable &b)
            a.penalty == b.penalty;
 }
 
-int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d_out)
+int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d_out, uint32_t part,
+           uint32_t nparts)
 {
     cudaStream_t s = ctx->stream;
     const uint32_t n = st->n;
@@ -1169,7 +1184,7 @@ int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d
     for(size_t i = 0; i < plans.size(); ++i) {
         NwPlan *c = plans[i];
         if(c->store_serial == st->serial && c->mode == mode && c->d_out == d_out && c->tiles.R == tiles.R &&
-           c->tiles.W == tiles.W && same_table(c->tbl, tbl)) {
+           c->tiles.W == tiles.W && c->part == part && c->nparts == nparts && same_table(c->tbl, tbl)) {
             pl = c;
             plans.erase(plans.begin() + i);
             plans.push_back(pl);
@@ -1179,7 +1194,7 @@ int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d
     if(!pl) {
         while(plans.size() >= kMaxPlans) { delete plans.front(); plans.erase(plans.begin()); }
         pl = new NwPlan;
-        const int rc = build_plan(ctx, st, tbl, mode, d_out, tiles, pl);
+        const int rc = build_plan(ctx, st, tbl, mode, d_out, tiles, part, nparts, pl);
         if(rc) { delete pl; return rc; }
         plans.push_back(pl);
     }

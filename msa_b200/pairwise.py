@@ -154,6 +154,46 @@ def score_units(flat: np.ndarray, offs: np.ndarray, lens: np.ndarray, table: Sco
     return out
 
 
+def part_of_pairs(flat: np.ndarray, offs: np.ndarray, lens: np.ndarray, table: ScoringTable,
+                  nparts: int) -> np.ndarray:
+    """The part (0..nparts-1) that scores each pair when a job is split over
+    `nparts` devices (msa_nw_part_of_pairs); host only, no device needed."""
+    n = len(lens)
+    flat = np.ascontiguousarray(flat, np.uint8)
+    offs = np.ascontiguousarray(offs, np.uint64)
+    lens = np.ascontiguousarray(lens, np.uint64)
+    out = np.zeros(max(n * (n - 1) // 2, 1), np.uint32)
+    check(lib().msa_nw_part_of_pairs(flat.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+                                     offs.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                                     lens.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)), n, ctypes.byref(table._t),
+                                     nparts, out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint32))))
+    return out[: n * (n - 1) // 2]
+
+
+def score_units_part(flat: np.ndarray, offs: np.ndarray, lens: np.ndarray, table: ScoringTable, part: int,
+                     nparts: int, out: np.ndarray | None = None, mode: int = MSA_NW_PERSISTENT,
+                     device: int | None = None) -> np.ndarray:
+    """Scores the pairs of one part (msa_nw_all_pairs_part) into `out` (host
+    int32 triangle; a zero-filled one if None); other entries are kept."""
+    ctx = runtime.context(device)
+    n = len(lens)
+    flat = np.ascontiguousarray(flat, np.uint8)
+    offs = np.ascontiguousarray(offs, np.uint64)
+    lens = np.ascontiguousarray(lens, np.uint64)
+    if out is None:
+        out = np.zeros(n * (n - 1) // 2, np.int32)
+    h = ctypes.c_uint64()
+    u8, u64 = ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint64)
+    check(lib().msa_seqs_upload(ctx.handle, flat.ctypes.data_as(u8), offs.ctypes.data_as(u64),
+                                lens.ctypes.data_as(u64), n, ctypes.byref(h)), ctx.handle)
+    try:
+        check(lib().msa_nw_all_pairs_part(ctx.handle, h.value, ctypes.byref(table._t), mode, part, nparts,
+                                          out.ctypes.data_as(ctypes.c_void_p), 0), ctx.handle)
+    finally:
+        lib().msa_seqs_release(ctx.handle, h.value)
+    return out
+
+
 def run(db: Database, table: Union[ScoringTable, str, None] = None,
         algorithm: Union[str, Callable] = "default", **kwargs) -> DistanceMatrix:
     """pairwise::run (src/pairwise/pairwise.cuh:231-244; src/python/pairwise.pyx:88-98)."""

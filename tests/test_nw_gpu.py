@@ -187,3 +187,61 @@ def test_repeated_call_replays_graph_with_identical_scores(gpu, tables):
     assert graphs == [1, 1, 1]
     want = oracle_scores(wl, "blosum62", tables)
     assert all(np.array_equal(o, want) for o in outs)
+
+
+def _split_workload():
+    # Uneven DNA lengths, plus sequences with END units inside (generic path).
+    rng = np.random.Generator(np.random.PCG64(21))
+    lens = W.c3_lengths(rng, 150, 0.75) // 4 + 50
+    seqs = [W._dna(rng, int(L)) for L in lens]
+    for k in (3, 77, 120):
+        s = np.array(seqs[k], np.uint8)
+        s[len(s) // 2] = ord("*")
+        seqs[k] = s
+    return W.Workload("split", seqs, "default", 21)
+
+
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("nparts", [2, 3])
+def test_parts_assemble_the_whole_matrix(gpu, mode, nparts):
+    wl = _split_workload()
+    flat, offs, lens = wl.flat_units()
+    table = ScoringTable(wl.table)
+    full = pairwise.score_units(flat, offs, lens, table, mode)
+    owner = pairwise.part_of_pairs(flat, offs, lens, table, nparts)
+    # Host output: each part writes only its own entries.
+    acc = np.full_like(full, 0x7eadbeef)
+    for p in range(nparts):
+        before = acc.copy()
+        pairwise.score_units_part(flat, offs, lens, table, p, nparts, out=acc, mode=mode)
+        changed = acc != before
+        assert not np.any(changed & (owner != p))
+        assert np.array_equal(acc[owner == p], full[owner == p])
+    assert np.array_equal(acc, full)
+
+
+def test_parts_on_device_into_one_buffer(gpu):
+    import torch
+
+    from msa_b200 import runtime, shard
+    wl = _split_workload()
+    flat, offs, lens = wl.flat_units()
+    table = ScoringTable(wl.table)
+    full = pairwise.score_units(flat, offs, lens, table)
+    ctx = runtime.context(0)
+    u8, u64 = ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint64)
+    h = ctypes.c_uint64()
+    _lib.check(_lib.lib().msa_seqs_upload(ctx.handle, flat.ctypes.data_as(u8), offs.ctypes.data_as(u64),
+                                          lens.ctypes.data_as(u64), wl.n, ctypes.byref(h)), ctx.handle)
+    try:
+        # Zero-filled partial triangles summed, as the multi-device exchange does.
+        total = torch.zeros(len(full), dtype=torch.int32, device="cuda:0")
+        for p in range(4):
+            part = torch.zeros_like(total)
+            torch.cuda.synchronize()   # the library scores on its own stream
+            shard.score_part(ctx, h.value, table, p, 4, part.data_ptr())
+            total += part
+        torch.cuda.synchronize()
+        assert np.array_equal(total.cpu().numpy(), full)
+    finally:
+        _lib.lib().msa_seqs_release(ctx.handle, h.value)
