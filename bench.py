@@ -363,6 +363,95 @@ def profile_run(args):
                       "launches": st.launches, "narrow_tasks": st.narrow_tasks}))
 
 
+def shard_bench(args):
+    """One c3 job split over all ranks (one GPU each): every rank scores its
+    part of equal DP cells into a zero-filled device triangle, and one NCCL
+    sum all-reduce assembles the whole matrix on every rank. Strong scaling:
+    the job is the same for any number of ranks. Timed per step from before
+    the part to after the exchange, max over ranks."""
+    import ctypes
+
+    import torch
+    import torch.distributed as dist
+
+    from msa_b200 import ScoringTable, _lib, runtime, shard
+    rank, world, local = _rank_info()
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=600))
+    lib = _lib.lib()
+    ctx = runtime.context(local)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    ctx.set_stream(stream.cuda_stream)
+    wl = load_workload(args.workload, 0)          # the same job on every rank
+    cfg = workload_config(args.workload, wl)
+    table = ScoringTable(wl.table)
+    flat, offs, lens = wl.flat_units()
+    n = wl.n
+    u8, u64 = ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint64)
+    h = ctypes.c_uint64()
+    _lib.check(lib.msa_seqs_upload(ctx.handle, flat.ctypes.data_as(u8), offs.ctypes.data_as(u64),
+                                   lens.ctypes.data_as(u64), n, ctypes.byref(h)), ctx.handle)
+    tri = torch.zeros(n * (n - 1) // 2, dtype=torch.int32, device=f"cuda:{local}")
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
+
+    def step():
+        tri.zero_()
+        shard.score_part(ctx, h.value, table, rank, world, tri.data_ptr())
+        if world > 1:
+            dist.all_reduce(tri, op=dist.ReduceOp.SUM)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    for _ in range(args.warmup):
+        step()
+    barrier()
+    sampler = ClockSampler(local)
+    sampler.start()
+    ms = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        step()
+        e1.record(stream)
+        e1.synchronize()
+        ms.append(e0.elapsed_time(e1))
+    barrier()
+    clocks = sampler.stop()
+    t = torch.tensor([float(np.mean(ms))], dtype=torch.float64, device=f"cuda:{local}")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    step_ms = float(t.item())
+    # Whole matrix on every rank: check it once against the one-device result.
+    ok = None
+    if rank == 0:
+        full = torch.empty_like(tri)
+        torch.cuda.synchronize()
+        _lib.check(lib.msa_nw_all_pairs(ctx.handle, h.value, ctypes.byref(table._t), _lib.MSA_NW_PERSISTENT,
+                                        ctypes.c_void_p(full.data_ptr()), 1), ctx.handle)
+        ok = bool(torch.equal(full, tri))
+        value = cfg["cells"] / (step_ms / 1e3) / 1e9
+        print(json.dumps({
+            "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": "int32/int16x2", "data": "synthetic (seeded)",
+            "config": dict(cfg, parallelism=f"one job split over {world} GPU(s): equal-cell parts, one NCCL "
+                                            f"sum all-reduce of the int32 triangle",
+                           l2="flushed (256 MB write) before every timed step"),
+            "matches_single_device": ok, "clocks": clocks}))
+    lib.msa_seqs_release(ctx.handle, h.value)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -374,6 +463,8 @@ def main():
     ap.add_argument("--cpu-cells", type=float, default=1.5e10)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-nj", action="store_true", help="skip the neighbor-joining leg")
+    ap.add_argument("--shard", action="store_true",
+                    help="one job split over all ranks with an NCCL exchange (strong scaling)")
     ap.add_argument("--profile", choices=["persistent", "plain", "nj"], default=None,
                     help="profiling run: --warmup calls then one call, on the first --n sequences")
     ap.add_argument("--n", type=int, default=0, help="with --profile: use the first N sequences")
@@ -388,6 +479,8 @@ def main():
         return serve_bench(args)
     if args.impl == "reference":
         return reference_arm(args)
+    if args.shard:
+        return shard_bench(args)
     if args.profile:
         return profile_run(args)
 
