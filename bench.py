@@ -629,6 +629,8 @@ def main():
             "gpu_launches": int(launches),
             "roofline": {"bound": "int32-issue", "achieved": kernel_gcups, "peak": peak, "unit": "GCUPS",
                          "frac": kernel_gcups / peak, "frac_x2": kernel_gcups / (2 * peak), "traffic": traffic,
+                         "ceilings_gcups": {"int32_lanes_alu": peak, "int16x2_lanes_alu": 2 * peak,
+                                            "int16x2_lanes_alu_plus_fma": 8 * peak / 3},
                          "peak_basis": f"{props.multi_processor_count} SM x 64 ALU lanes/clk x {sm_mhz:.0f} MHz "
                                        f"(median sampled) / 2 max-ops per cell (int32 lanes); frac_x2 is against "
                                        f"the 16x2-lane ceiling, twice that"},

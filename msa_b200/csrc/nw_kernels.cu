@@ -22,6 +22,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 
 #include "msa_internal.hpp"
 
@@ -71,17 +72,22 @@ struct Wide {
     __device__ static __forceinline__ W cell_chain(W up, W ng, W part) { return __viaddmax_s32(up, ng, part); }
 };
 
+// Two cells per 32-bit lane (16-bit halves: the two rows sequences of a rows
+// pair). The lane state is not H but S = H - g + 0x8000 per half, and the
+// staged score words hold s + g, so a cell is
+//     S = vimax3_u16x2(S_left, S_up, S_diag + (s + g)) - g
+// one three-way max (ALU pipe), one vadd2 (FMA pipe) and one 32-bit subtract
+// that the compiler may place on either pipe: the two integer pipes share the
+// work, where max(up - g, max(left - g, diag + s)) as two DPX maxes puts two
+// ALU operations on every cell. The 0x8000 bias keeps every half at or above
+// g (the 16-bit bound narrow_ok proves), so the 32-bit subtract never borrows
+// across halves, and the unsigned three-way max orders biased values exactly.
 struct Narrow {
     using W = uint32_t;
-    __device__ static __forceinline__ W cell(W d, W s, W left, W up, W ng)
-    {
-        const W ds = __vadd2(d, s);
-        const W t = __viaddmax_s16x2(left, ng, ds);
-        return __viaddmax_s16x2(up, ng, t);
-    }
+    __device__ static __forceinline__ W state(int32_t h, int32_t g) { return ((uint32_t) (h - g + 0x8000) & 0xffffu) * 0x10001u; }
+    __device__ static __forceinline__ int32_t lo(W w, int32_t g) { return (int32_t) (w & 0xffffu) - 0x8000 + g; }
+    __device__ static __forceinline__ int32_t hi(W w, int32_t g) { return (int32_t) (w >> 16) - 0x8000 + g; }
     __device__ static __forceinline__ W splat(int32_t v) { return dup16(v); }
-    __device__ static __forceinline__ W cell_part(W d, W s, W left, W ng) { return __viaddmax_s16x2(left, ng, __vadd2(d, s)); }
-    __device__ static __forceinline__ W cell_chain(W up, W ng, W part) { return __viaddmax_s16x2(up, ng, part); }
 };
 
 // R profile bytes of one lane for residue code b, from the staged strip.
@@ -409,12 +415,13 @@ namespace dev {
 // Stages strip rows [i0, i0 + 32R) as 32-bit profile words in shared memory,
 // laid out [code][plane of 4 rows][lane][4 words] so that one 16-byte load per
 // lane and plane is bank-conflict free for any codes the lanes hold.
-// Narrow: word = (s(X1_i, b), s(X2_i, b)) as int16x2; rows of X2 past its
-// profile (lp2) read as 0. Wide: word = s(X1_i, b) as int32.
+// Narrow: word = (s(X1_i, b) + g, s(X2_i, b) + g) as int16x2; rows of X2 past
+// its profile (lp2) score 0. Wide: word = s(X1_i, b) as int32.
 template <int R, bool kNarrow>
 __device__ __forceinline__ void stage_words(uint32_t *sprof, const int8_t *__restrict__ g1, uint32_t lp1,
-                                            const int8_t *__restrict__ g2, uint32_t lp2, int i0)
+                                            const int8_t *__restrict__ g2, uint32_t lp2, int i0, int32_t gap = 0)
 {
+    const uint32_t gg = ((uint32_t) gap & 0xffffu) * 0x10001u;
     constexpr int SH = 32 * R;
     constexpr int G = SH / 4;        // 4-row groups per code row
     constexpr int PL = R / 4;        // planes per lane
@@ -426,10 +433,10 @@ __device__ __forceinline__ void stage_words(uint32_t *sprof, const int8_t *__res
         if constexpr(kNarrow) {
             uint32_t vb = 0;
             if((uint32_t) (i0 + 4 * rg) < lp2) vb = __ldg(reinterpret_cast<const uint32_t *>(g2 + (size_t) b * lp2 + i0) + rg);
-            o.x = sbyte2<0>(va, vb);
-            o.y = sbyte2<1>(va, vb);
-            o.z = sbyte2<2>(va, vb);
-            o.w = sbyte2<3>(va, vb);
+            o.x = __vadd2(sbyte2<0>(va, vb), gg);
+            o.y = __vadd2(sbyte2<1>(va, vb), gg);
+            o.z = __vadd2(sbyte2<2>(va, vb), gg);
+            o.w = __vadd2(sbyte2<3>(va, vb), gg);
         } else {
             o.x = (uint32_t) sbyte<0>(va);
             o.y = (uint32_t) sbyte<1>(va);
@@ -446,8 +453,9 @@ template <bool V> struct Guard { static constexpr bool value = V; };
 // warp. `bound` holds the row above the strip on entry (column j at index j)
 // and, when store_bound, the strip's last row on exit. After the call, lane k's
 // H registers hold the strip's rows at the last column it reached
-// (tend - 1 - lane). Steps run in groups of 4; only the fill and drain groups,
-// where some lanes sit outside [0, ncols), test the lane's column.
+// (tend - 1 - lane). Steps run in groups of 8 (the loop bookkeeping of a group
+// is shared by 8 columns); only the fill and drain groups, where some lanes
+// sit outside [0, ncols), test the lane's column.
 template <int R, class K>
 __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, const uint8_t *__restrict__ cols,
                                             int ncols, uint32_t *__restrict__ bound, int i0, int tend,
@@ -455,10 +463,19 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
 {
     using W = typename K::W;
     constexpr int SH = 32 * R;
+    constexpr bool kB = std::is_same<K, Narrow>::value;
     const W ng = K::splat(-g);
+    W diag;
+    if constexpr(kB) {
 #pragma unroll
-    for(int r = 0; r < R; ++r) H[r] = K::splat(-(i0 + lane * R + r + 1) * g);
-    W diag = K::splat(-(i0 + lane * R) * g);
+        for(int r = 0; r < R; ++r) H[r] = Narrow::state(-(i0 + lane * R + r + 1) * g, g);
+        diag = Narrow::state(-(i0 + lane * R) * g, g);
+    } else {
+#pragma unroll
+        for(int r = 0; r < R; ++r) H[r] = K::splat(-(i0 + lane * R + r + 1) * g);
+        diag = K::splat(-(i0 + lane * R) * g);
+    }
+    const W g2 = ((uint32_t) g & 0xffffu) * 0x10001u;
     W hlast = H[R - 1];
     uint32_t bq_cur = bound[lane], bq_nxt = bound[32 + lane];
     const uint32_t *prow = sprof + lane * 4;
@@ -473,7 +490,7 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
             bq_nxt = bound[t0 + 32 + lane];
         }
 #pragma unroll
-        for(int u = 0; u < 4; ++u) {
+        for(int u = 0; u < 8; ++u) {
             W up = __shfl_up_sync(kFull, hlast, 1);
             const uint32_t bv = __shfl_sync(kFull, bq_cur, (t0 & 31) + u);
             if(lane == 0) up = (W) bv;
@@ -481,6 +498,21 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
                 const uint32_t *pb = prow + cur * SH;
                 uint4 pw = *reinterpret_cast<const uint4 *>(pb);
                 W sc[4] = {(W) pw.x, (W) pw.y, (W) pw.z, (W) pw.w};
+                if constexpr(kB) {
+                    // S = max(S_left, S_up, S_diag + s + g) - g, per half (see Narrow).
+                    W above = up, dprev = diag;
+#pragma unroll
+                    for(int r = 0; r < R; ++r) {
+                        if(r > 0 && (r & 3) == 0) {
+                            pw = *reinterpret_cast<const uint4 *>(pb + (r >> 2) * 128);
+                            sc[0] = (W) pw.x; sc[1] = (W) pw.y; sc[2] = (W) pw.z; sc[3] = (W) pw.w;
+                        }
+                        const W D = __vadd2(dprev, sc[r & 3]);
+                        dprev = H[r];
+                        H[r] = __vimax3_u16x2(H[r], above, D) - g2;
+                        above = H[r];
+                    }
+                } else {
                 // Row r needs the old H[r-1] (diagonal) and old H[r] (left): the
                 // off-chain part for row r+1 is computed before row r is
                 // overwritten, so no register copies are needed.
@@ -499,6 +531,7 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
                     H[r] = K::cell_chain(u_, ng, pr);
                     u_ = H[r];
                 }
+                }
                 hlast = H[R - 1];
                 if(st31) bound[j] = (uint32_t) hlast;
                 diag = up;
@@ -509,14 +542,14 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
         }
     };
 
-    const int tend4 = (tend + 3) & ~3;
+    const int tend4 = (tend + 7) & ~7;
     int t0 = 0;
 #pragma unroll 1
-    for(; t0 < tend4 && t0 < 32; t0 += 4) group(t0, Guard<true>{});
+    for(; t0 < tend4 && t0 < 32; t0 += 8) group(t0, Guard<true>{});
 #pragma unroll 1
-    for(; t0 + 3 < ncols; t0 += 4) group(t0, Guard<false>{});   // every lane inside [0, ncols)
+    for(; t0 + 7 < ncols; t0 += 8) group(t0, Guard<false>{});   // every lane inside [0, ncols)
 #pragma unroll 1
-    for(; t0 < tend4; t0 += 4) group(t0, Guard<true>{});
+    for(; t0 < tend4; t0 += 8) group(t0, Guard<true>{});
 }
 
 template <int R, class K>
@@ -539,7 +572,7 @@ __device__ __noinline__ void narrow_task(uint32_t *sprof, const int8_t *g1, uint
     for(int s = 0; s < nst; ++s) {
         const int i0 = s * SH;
         __syncthreads();
-        stage_words<R, true>(sprof, g1, lp1, g2, lp2, i0);
+        stage_words<R, true>(sprof, g1, lp1, g2, lp2, i0, g);
         __syncthreads();
         if(has) {
             const bool last = s == nst - 1;
@@ -550,11 +583,11 @@ __device__ __noinline__ void narrow_task(uint32_t *sprof, const int8_t *g1, uint
             __syncwarp();
             if(s == s2) {
                 const int rr = e2 - 1 - i0;
-                r2 = __shfl_sync(kFull, hi16(pick_row<R, Narrow>(H, rr % R)), rr / R);
+                r2 = __shfl_sync(kFull, Narrow::hi(pick_row<R, Narrow>(H, rr % R), g), rr / R);
             }
             if(last) {
                 const int rr = e1 - 1 - i0;
-                r1 = __shfl_sync(kFull, lo16(pick_row<R, Narrow>(H, rr % R)), rr / R);
+                r1 = __shfl_sync(kFull, Narrow::lo(pick_row<R, Narrow>(H, rr % R), g), rr / R);
             }
         }
     }
@@ -619,7 +652,7 @@ __device__ __forceinline__ void rows_pair_task(const JobView &jv, uint32_t k, ui
 
     if(jv.row_narrow[k]) {
         // Row zero of the DP as the boundary above the first strip.
-        if(has) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = dev::dup16(-(jj + 1) * jv.g);
+        if(has) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = dev::Narrow::state(-(jj + 1) * jv.g, jv.g);
         int nst, R;
         dev::strip_plan<RMAX>(e1, nst, R);
         int32_t r1 = 0, r2 = 0;
