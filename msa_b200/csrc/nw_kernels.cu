@@ -73,15 +73,21 @@ struct Wide {
 };
 
 // Two cells per 32-bit lane (16-bit halves: the two rows sequences of a rows
-// pair). The lane state is not H but S = H - g + 0x8000 per half, and the
-// staged score words hold s + g, so a cell is
-//     S = vimax3_u16x2(S_left, S_up, S_diag + (s + g)) - g
-// one three-way max (ALU pipe), one vadd2 (FMA pipe) and one 32-bit subtract
-// that the compiler may place on either pipe: the two integer pipes share the
-// work, where max(up - g, max(left - g, diag + s)) as two DPX maxes puts two
-// ALU operations on every cell. The 0x8000 bias keeps every half at or above
-// g (the 16-bit bound narrow_ok proves), so the 32-bit subtract never borrows
-// across halves, and the unsigned three-way max orders biased values exactly.
+// pair). The lane state is not H but S = H - g + 0x8000 per half, in which a
+// cell is S = max(S_left - g, S_up - g, S_diag + s), computed in one of two
+// forms:
+//   two maxes:       max(S_up - g, max(S_left - g, S_diag + s))
+//                    two viaddmax_u16x2 (ALU) and a vadd2 (FMA); one dependent
+//                    operation on the chain down a lane's rows;
+//   three-way max:   vimax3_u16x2(S_left, S_up, S_diag + (s + g)) - g
+//                    one ALU max, a vadd2 and a 32-bit subtract either integer
+//                    pipe may take; two dependent operations on the chain.
+// Even rows of a lane take the first form and odd rows the second (the staged
+// words hold s or s + g accordingly), which spreads the work over both integer
+// pipes while keeping the row chain short. The 0x8000 bias keeps every half at
+// or above g under the 16-bit bound narrow_ok proves, so the 32-bit subtract
+// never borrows across halves, the unsigned maxes order biased values exactly,
+// and S - g never wraps.
 struct Narrow {
     using W = uint32_t;
     __device__ static __forceinline__ W state(int32_t h, int32_t g) { return ((uint32_t) (h - g + 0x8000) & 0xffffu) * 0x10001u; }
@@ -415,8 +421,9 @@ namespace dev {
 // Stages strip rows [i0, i0 + 32R) as 32-bit profile words in shared memory,
 // laid out [code][plane of 4 rows][lane][4 words] so that one 16-byte load per
 // lane and plane is bank-conflict free for any codes the lanes hold.
-// Narrow: word = (s(X1_i, b) + g, s(X2_i, b) + g) as int16x2; rows of X2 past
-// its profile (lp2) score 0. Wide: word = s(X1_i, b) as int32.
+// Narrow: word = (s(X1_i, b), s(X2_i, b)) as int16x2, plus g in both halves on
+// odd rows of a lane; rows of X2 past its profile (lp2) score 0. Wide: word =
+// s(X1_i, b) as int32.
 template <int R, bool kNarrow>
 __device__ __forceinline__ void stage_words(uint32_t *sprof, const int8_t *__restrict__ g1, uint32_t lp1,
                                             const int8_t *__restrict__ g2, uint32_t lp2, int i0, int32_t gap = 0)
@@ -433,9 +440,11 @@ __device__ __forceinline__ void stage_words(uint32_t *sprof, const int8_t *__res
         if constexpr(kNarrow) {
             uint32_t vb = 0;
             if((uint32_t) (i0 + 4 * rg) < lp2) vb = __ldg(reinterpret_cast<const uint32_t *>(g2 + (size_t) b * lp2 + i0) + rg);
-            o.x = __vadd2(sbyte2<0>(va, vb), gg);
+            // Even rows of a lane take the two-max form (score s), odd rows
+            // the three-way-max form (score s + g); see Narrow.
+            o.x = sbyte2<0>(va, vb);
             o.y = __vadd2(sbyte2<1>(va, vb), gg);
-            o.z = __vadd2(sbyte2<2>(va, vb), gg);
+            o.z = sbyte2<2>(va, vb);
             o.w = __vadd2(sbyte2<3>(va, vb), gg);
         } else {
             o.x = (uint32_t) sbyte<0>(va);
@@ -476,6 +485,7 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
         diag = K::splat(-(i0 + lane * R) * g);
     }
     const W g2 = ((uint32_t) g & 0xffffu) * 0x10001u;
+    const W ng16 = ((uint32_t) (-g) & 0xffffu) * 0x10001u;
     W hlast = H[R - 1];
     uint32_t bq_cur = bound[lane], bq_nxt = bound[32 + lane];
     const uint32_t *prow = sprof + lane * 4;
@@ -499,7 +509,8 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
                 uint4 pw = *reinterpret_cast<const uint4 *>(pb);
                 W sc[4] = {(W) pw.x, (W) pw.y, (W) pw.z, (W) pw.w};
                 if constexpr(kB) {
-                    // S = max(S_left, S_up, S_diag + s + g) - g, per half (see Narrow).
+                    // Alternate rows: two maxes (one dependent op on the row
+                    // chain) and the three-way max (one ALU op); see Narrow.
                     W above = up, dprev = diag;
 #pragma unroll
                     for(int r = 0; r < R; ++r) {
@@ -509,7 +520,8 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
                         }
                         const W D = __vadd2(dprev, sc[r & 3]);
                         dprev = H[r];
-                        H[r] = __vimax3_u16x2(H[r], above, D) - g2;
+                        if(r % 2 == 0) H[r] = __viaddmax_u16x2(above, ng16, __viaddmax_u16x2(H[r], ng16, D));
+                        else H[r] = __vimax3_u16x2(H[r], above, D) - g2;
                         above = H[r];
                     }
                 } else {
@@ -817,13 +829,16 @@ static int occupancy(KernelT kernel, size_t smem, int *blocks)
     return 0;
 }
 
-// 16-bit lanes are exact when every value a task can produce fits int16:
+// 16-bit lanes are exact when every value a task can produce fits them:
 // H(i,j) lies in [-g(i+j), max(smax,0)*min(i,j)] for all i <= rows (padded
-// strip rows included, whose scores are 0) and j <= cols, and the two partial
-// sums (diag + s, left - g) reach at most max(g, |smin|) below the floor.
+// strip rows included, whose scores are 0) and j <= cols, and the partial sums
+// (diag + s, left - g) reach at most max(g, |smin|) below the floor. The lane
+// state S = H - g + 0x8000 and the two-max form's S_diag + s must stay in
+// [0, 0xffff] with S >= g, which costs one more g of headroom below:
+// g(rows + cols) + g + max(g, |smin|) <= 32768.
 static inline bool narrow_ok(int64_t rows_p, int64_t cols, const ExtTable &t)
 {
-    const int64_t lo = (int64_t) t.penalty * (rows_p + cols) + std::max<int64_t>(t.penalty, t.max_neg);
+    const int64_t lo = (int64_t) t.penalty * (rows_p + cols + 1) + std::max<int64_t>(t.penalty, t.max_neg);
     const int64_t hi = (int64_t) std::max<int32_t>(t.max_pos, 0) * std::min(rows_p, cols);
     return lo <= 32768 && hi <= 32767;
 }

@@ -245,3 +245,25 @@ def test_parts_on_device_into_one_buffer(gpu):
         assert np.array_equal(total.cpu().numpy(), full)
     finally:
         _lib.lib().msa_seqs_release(ctx.handle, h.value)
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_16bit_lanes_near_their_bound(gpu, golden, mode):
+    # Gaps cost 1 and mismatches 60, so an all-A against an all-C sequence is
+    # scored by the all-gap path: H at the far corner is -(L1 + L2), within a
+    # few hundred of the 16-bit lanes' floor; the batched kernel must still
+    # take them (narrow_tasks) and stay exact. A longer pair must fall back to
+    # 32-bit lanes.
+    m = np.full((25, 25), -60, np.int32)
+    np.fill_diagonal(m, 1)
+    table = ScoringTable.custom(m, 1)
+    for la, lc, narrow in ((16380, 15999, True), (16383, 16383, False)):
+        seqs = [b"A" * la, b"C" * lc, b"A" * (lc - 3)]
+        wl = W.Workload("edge", [np.frombuffer(s, np.uint8) for s in seqs], "default", 0)
+        flat, offs, lens = wl.flat_units()
+        got = pairwise.score_units(flat, offs, lens, table, mode)
+        # (1,0): all gaps; (2,0): lc-3 matches then la-(lc-3) gaps; (2,1): all gaps
+        want = np.array([-(la + lc), (lc - 3) - (la - (lc - 3)), -(lc + lc - 3)], np.int32)
+        assert np.array_equal(got, want), (la, lc, got, want)
+        if mode == _lib.MSA_NW_PERSISTENT:
+            assert (pairwise.last_stats().narrow_tasks > 0) == narrow
