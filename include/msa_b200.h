@@ -118,6 +118,26 @@ int msa_seqs_release(msa_ctx *ctx, msa_seqs seqs);
 /* Number of sequences in a store, or -1 for a bad handle. */
 int64_t msa_seqs_count(msa_ctx *ctx, msa_seqs seqs);
 
+/*
+ * FASTA files straight into a device store: the reference's loader
+ * (io::loader by extension, src/io/loader/database.cpp:31-52; parser::fasta,
+ * src/io/loader/parser/fasta.cpp:26-70; encoder::encode, src/encoder.cpp:46-57)
+ * in one pass per file, then one upload. Records keep the reference's rules:
+ * contents are the lines after a '>' line up to the next '>' line or the first
+ * empty line, '\r' stays (and encodes as END), only "fa"/"fasta" files are read.
+ * *count receives the number of records; their descriptions stay with the store
+ * (msa_seqs_description).
+ */
+int msa_seqs_load_fasta(msa_ctx *ctx, const char *const *files, uint32_t nfiles, msa_seqs *out, uint32_t *count);
+/* Description of record `index` of a store made by msa_seqs_load_fasta, valid
+ * until the store is released; NULL otherwise. */
+const char *msa_seqs_description(msa_ctx *ctx, msa_seqs seqs, uint32_t index);
+/* Host-only halves of the same loader: the record count and total units, then
+ * the units (one byte each, unpadded), offsets and lengths, as msa_seqs_upload
+ * takes them. */
+int msa_fasta_count(const char *const *files, uint32_t nfiles, uint32_t *nseqs, uint64_t *nunits);
+int msa_fasta_encode(const char *const *files, uint32_t nfiles, uint8_t *units, uint64_t *offs, uint64_t *lens);
+
 /* ---------------------------------------------------------- all-pairs NW */
 
 typedef enum msa_nw_mode {

@@ -84,6 +84,31 @@ class database
     std::vector<std::pair<std::string, size_t>> m_index;
 };
 
+/* Sequences resident on the current device (a store of msa_seqs_load_fasta),
+ * with their descriptions: the fast path from FASTA files to the pairwise
+ * step, with no host database in between. */
+class device_database
+{
+  public:
+    device_database() = default;
+    device_database(const device_database &) = delete;
+    device_database &operator=(const device_database &) = delete;
+    device_database(device_database &&o) noexcept { *this = std::move(o); }
+    device_database &operator=(device_database &&o) noexcept;
+    ~device_database();
+    size_t count() const { return m_count; }
+    int device() const { return m_device; }
+    msa_seqs handle() const { return m_handle; }
+    const std::vector<std::string> &descriptions() const { return m_names; }
+
+  private:
+    friend device_database load_to_device_impl(const std::vector<std::string> &);
+    int m_device = -1;
+    msa_seqs m_handle = 0;
+    size_t m_count = 0;
+    std::vector<std::string> m_names;
+};
+
 namespace io {
 /* parser::fasta: records from '>' lines; a record's contents are the lines up
  * to the next '>' line or the first empty line. */
@@ -91,6 +116,9 @@ database fasta(const std::string &filename);
 /* The loader by file extension ("fa", "fasta"); throws "unknown database
  * parser '<ext>'" otherwise. Files are merged in order. */
 database load(const std::vector<std::string> &filenames);
+/* The same files parsed, encoded and uploaded in one pass onto the current
+ * device (msa_seqs_load_fasta). */
+device_database load_to_device(const std::vector<std::string> &filenames);
 }  // namespace io
 
 /* The devices the facade runs on (cuda::device in the reference). */
@@ -161,6 +189,8 @@ struct algorithm {
  * on the current device. */
 distance_matrix run(const database &db, const scoring_table &table, const std::string &algorithm = "default",
                     int devices = 1);
+/* pairwise::run over sequences already resident on a device. */
+distance_matrix run(const device_database &db, const scoring_table &table, const std::string &algorithm = "default");
 
 }  // namespace pairwise
 

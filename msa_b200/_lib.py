@@ -120,6 +120,14 @@ _PROTOS = [
                                             ctypes.POINTER(ctypes.c_uint64), ctypes.c_uint32, ctypes.POINTER(MsaTable),
                                             ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]),
     ("msa_nw_set_tiles", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    ("msa_seqs_load_fasta", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_char_p), ctypes.c_uint32,
+                                           ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint32)]),
+    ("msa_seqs_description", ctypes.c_char_p, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32]),
+    ("msa_fasta_count", ctypes.c_int, [ctypes.POINTER(ctypes.c_char_p), ctypes.c_uint32,
+                                       ctypes.POINTER(ctypes.c_uint32), ctypes.POINTER(ctypes.c_uint64)]),
+    ("msa_fasta_encode", ctypes.c_int, [ctypes.POINTER(ctypes.c_char_p), ctypes.c_uint32,
+                                        ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint64),
+                                        ctypes.POINTER(ctypes.c_uint64)]),
     ("msa_nw_all_pairs_noalloc", ctypes.c_int, [ctypes.c_void_p, c_u64p, c_u64p, ctypes.c_uint32,
                                                 ctypes.POINTER(MsaTable), ctypes.c_void_p, ctypes.c_void_p]),
     ("msa_noalloc_last_error", ctypes.c_char_p, []),

@@ -18,7 +18,7 @@ BUILD_DIR = PKG / "_build"
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 SOURCES = ["tables.cpp", "abi.cpp", "partition.cpp", "nw_kernels.cu", "nj_kernel.cu", "probe.cu", "noalloc.cu",
-           "serve.cpp", "facade.cu"]
+           "serve.cpp", "facade.cu", "fasta.cpp"]
 # The command line (museqa), linked against the library.
 CLI = PKG / "museqa"
 CLI_SOURCE = "cli.cpp"

@@ -127,20 +127,32 @@ try {
     device::select(cmd.has("gpu-id") ? std::stoi(cmd.get("gpu-id", "0")) % ndev : 0);
     const int devices = cmd.has("multigpu") ? ndev : 1;
 
-    // loading
+    // loading: one device goes straight from the files to a device store;
+    // several devices take the host database and split the job.
     auto t0 = std::chrono::steady_clock::now();
-    const database db = io::load(cmd.positional);
-    if(db.count() > 0) watchdog::info("loaded a total of <bold>" + std::to_string(db.count()) + "</> sequences");
+    database host_db;
+    device_database dev_db;
+    std::vector<std::string> names;
+    if(devices > 1) {
+        host_db = io::load(cmd.positional);
+        for(const auto &e : host_db) names.push_back(e.description);
+    } else {
+        dev_db = io::load_to_device(cmd.positional);
+        names = dev_db.descriptions();
+    }
+    const size_t count = names.size();
+    if(count > 0) watchdog::info("loaded a total of <bold>" + std::to_string(count) + "</> sequences");
     watchdog::report("loading", seconds_since(t0));
 
     // pairwise
     t0 = std::chrono::steady_clock::now();
     watchdog::info("chosen pairwise algorithm <bold>" + pw_algo + "</>");
     watchdog::info("chosen pairwise scoring table <bold>" + table_name + "</>");
-    const unsigned long long npairs = (unsigned long long) db.count() * (db.count() ? db.count() - 1 : 0) / 2;
+    const unsigned long long npairs = (unsigned long long) count * (count ? count - 1 : 0) / 2;
     watchdog::init("pairwise", "aligning <bold>" + std::to_string(npairs) + "</> pairs");
+    const auto table = pairwise::scoring_table::make(table_name);
     const pairwise::distance_matrix dm =
-        pairwise::run(db, pairwise::scoring_table::make(table_name), pw_algo, devices);
+        devices > 1 ? pairwise::run(host_db, table, pw_algo, devices) : pairwise::run(dev_db, table, pw_algo);
     watchdog::finish("pairwise", "aligned all sequence pairs");
     watchdog::report("pairwise", seconds_since(t0));
 
@@ -148,7 +160,7 @@ try {
     t0 = std::chrono::steady_clock::now();
     watchdog::info("chosen phylogeny algorithm <bold>" + pg_algo + "</>");
     watchdog::init("phylogeny", "producing phylogenetic tree");
-    const phylogeny::guidetree tree = phylogeny::run(dm, db.count(), pg_algo);
+    const phylogeny::guidetree tree = phylogeny::run(dm, count, pg_algo);
     watchdog::finish("phylogeny", "phylogenetic tree produced");
     watchdog::report("phylogeny", seconds_since(t0));
 
@@ -156,8 +168,6 @@ try {
     watchdog::warning("the profile-aligner module is not part of this build; the pipeline ends at the guide tree");
 
     if(cmd.has("newick")) {
-        std::vector<std::string> names;
-        for(const auto &e : db) names.push_back(e.description);
         std::ofstream f(cmd.get("newick", ""));
         if(!f) throw exception("cannot write '" + cmd.get("newick", "") + "'");
         f << tree.newick(names) << "\n";

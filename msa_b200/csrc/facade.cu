@@ -209,6 +209,51 @@ int current() { return t_device; }
 
 }  // namespace device
 
+device_database &device_database::operator=(device_database &&o) noexcept
+{
+    if(this != &o) {
+        std::swap(m_device, o.m_device);
+        std::swap(m_handle, o.m_handle);
+        std::swap(m_count, o.m_count);
+        std::swap(m_names, o.m_names);
+    }
+    return *this;
+}
+
+device_database::~device_database()
+{
+    if(m_handle && m_device >= 0) {
+        cudaSetDevice(m_device);
+        msa_seqs_release(context_for(m_device), m_handle);
+    }
+}
+
+device_database load_to_device_impl(const std::vector<std::string> &filenames)
+{
+    device_database db;
+    const int dev = device::current();
+    msa_ctx *c = context_for(dev);
+    check_cuda(cudaSetDevice(dev), "select device");
+    std::vector<const char *> names;
+    for(const auto &f : filenames) names.push_back(f.c_str());
+    uint32_t n = 0;
+    msa_seqs h = 0;
+    const int rc = msa_seqs_load_fasta(c, names.data(), (uint32_t) names.size(), &h, &n);
+    if(rc) throw exception(msa_last_error(c) && *msa_last_error(c) ? msa_last_error(c) : msa_strerror(rc));
+    db.m_device = dev;
+    db.m_handle = h;
+    db.m_count = n;
+    for(uint32_t k = 0; k < n; ++k) {
+        const char *d = msa_seqs_description(c, h, k);
+        db.m_names.emplace_back(d ? d : "");
+    }
+    return db;
+}
+
+namespace io {
+device_database load_to_device(const std::vector<std::string> &filenames) { return load_to_device_impl(filenames); }
+}  // namespace io
+
 // ------------------------------------------------------------------ pairwise
 
 namespace pairwise {
@@ -428,6 +473,23 @@ std::vector<std::string> algorithm::list()
     std::vector<std::string> out;
     for(const auto &p : pairwise_names()) out.push_back(p.first);
     return out;
+}
+
+distance_matrix run(const device_database &db, const scoring_table &table, const std::string &name)
+{
+    int mode = -1;
+    for(const auto &p : pairwise_names())
+        if(p.first == name) mode = p.second;
+    if(mode < 0) throw exception(format("unknown pairwise algorithm '%s'", name.c_str()));
+    const size_t n = db.count();
+    const uint64_t np = (uint64_t) n * (n ? n - 1 : 0) / 2;
+    auto st = std::make_shared<distance_matrix::storage>();
+    st->device = db.device();
+    check_cuda(cudaSetDevice(db.device()), "select device");
+    check_cuda(cudaMalloc((void **) &st->dev, std::max<uint64_t>(np * 4, 16)), "allocate distance matrix");
+    msa_ctx *c = context_for(db.device());
+    check_status(msa_nw_all_pairs(c, db.handle(), &table.raw(), mode, st->dev, 1), c);
+    return make_device_matrix(st, n);
 }
 
 distance_matrix run(const database &db, const scoring_table &table, const std::string &name, int devices)

@@ -70,6 +70,7 @@ struct SeqStore {
     uint64_t prof_bytes = 0;
     uint64_t *d_prof_off = nullptr;
     uint32_t *d_prof_lp = nullptr;
+    std::vector<std::string> names;   // record descriptions (msa_seqs_load_fasta)
 };
 
 // Growable device scratch buffer owned by a context.

@@ -71,6 +71,59 @@ def test_cpp_fasta_loader_equals_python(tmp_path, fasta_dump, name):
     assert got == want
 
 
+def _fast_path_units(files):
+    import ctypes
+    from msa_b200 import _lib
+    lib = _lib.lib()
+    arr = (ctypes.c_char_p * len(files))(*[str(f).encode() for f in files])
+    ns, nu = ctypes.c_uint32(), ctypes.c_uint64()
+    rc = lib.msa_fasta_count(arr, len(files), ctypes.byref(ns), ctypes.byref(nu))
+    if rc:
+        return rc, None
+    units = np.zeros(max(nu.value, 1), np.uint8)
+    offs = np.zeros(max(ns.value, 1), np.uint64)
+    lens = np.zeros(max(ns.value, 1), np.uint64)
+    rc = lib.msa_fasta_encode(arr, len(files), units.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)),
+                              offs.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)),
+                              lens.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64)))
+    return rc, [units[int(o):int(o + n)] for o, n in zip(offs[:ns.value], lens[:ns.value])]
+
+
+def test_fast_fasta_loader_equals_python(tmp_path):
+    # The one-pass loader behind msa_seqs_load_fasta, on every awkward case
+    # at once (files are merged in order, as the reference's loader does).
+    files = []
+    for name, data in sorted(FASTA_CASES.items()):
+        f = tmp_path / name
+        f.write_bytes(data)
+        files.append(f)
+    rc, got = _fast_path_units(files)
+    assert rc == 0
+    db = Database.load(*map(str, files))
+    want = [e.contents.units[:e.contents.raw_length] for e in db]
+    assert len(got) == len(want)
+    assert all(np.array_equal(a, b) for a, b in zip(got, want))
+
+
+def test_fast_fasta_loader_on_the_reference_databases():
+    db_dir = Path("/root/reference/db")
+    files = sorted(db_dir.glob("*.fasta")) if db_dir.is_dir() else []
+    if not files:
+        pytest.skip("the reference's FASTA databases are not present")
+    for f in files[:6]:
+        rc, got = _fast_path_units([f])
+        assert rc == 0
+        want = [e.contents.units[:e.contents.raw_length] for e in Database.load(str(f))]
+        assert len(got) == len(want) and all(np.array_equal(a, b) for a, b in zip(got, want)), f.name
+
+
+def test_fast_fasta_loader_errors(tmp_path):
+    f = tmp_path / "x.txt"
+    f.write_text(">a\nAC\n")
+    assert _fast_path_units([f])[0] != 0
+    assert _fast_path_units([tmp_path / "missing.fasta"])[0] != 0
+
+
 def test_cpp_loader_rejects_unknown_extension(tmp_path, fasta_dump):
     f = tmp_path / "seqs.txt"
     f.write_text(">a\nAC\n")
@@ -126,3 +179,29 @@ def test_report_only_prints_only_reports(gpu, tmp_path):
     assert rc == 0
     events = {ln.split("|")[1] for ln in out.splitlines()}
     assert events <= {"report", "warning"}
+
+
+@pytest.mark.gpu
+def test_fasta_straight_to_device_store(gpu, tmp_path):
+    import ctypes
+    from msa_b200 import _lib, runtime
+    wl = W.random_set(32, 30, 20, 300)
+    fasta = tmp_path / "s.fasta"
+    fasta.write_bytes(b"".join(b">seq %d\r\n%s\n" % (k, bytes(s)) for k, s in enumerate(wl.seqs)))
+    ctx = runtime.context(0)
+    lib = _lib.lib()
+    arr = (ctypes.c_char_p * 1)(str(fasta).encode())
+    h, n = ctypes.c_uint64(), ctypes.c_uint32()
+    _lib.check(lib.msa_seqs_load_fasta(ctx.handle, arr, 1, ctypes.byref(h), ctypes.byref(n)), ctx.handle)
+    try:
+        db = Database.load(str(fasta))
+        assert n.value == db.count
+        assert [lib.msa_seqs_description(ctx.handle, h.value, k).decode("latin-1") for k in range(n.value)] == \
+               [e.description for e in db]
+        out = np.zeros(n.value * (n.value - 1) // 2, np.int32)
+        t = ScoringTable("blosum62")
+        _lib.check(lib.msa_nw_all_pairs(ctx.handle, h.value, ctypes.byref(t._t), _lib.MSA_NW_PERSISTENT,
+                                        out.ctypes.data_as(ctypes.c_void_p), 0), ctx.handle)
+        assert np.array_equal(out, pairwise.run(db, t).int_scores)
+    finally:
+        lib.msa_seqs_release(ctx.handle, h.value)
