@@ -282,7 +282,16 @@ typedef struct msa_serve_config {
     int device;
     uint64_t hbm_budget_bytes;  /* 0 = 80 % of free device memory at start */
     uint32_t max_jobs;          /* admitted jobs at once; 0 = 64 */
-    uint32_t quantum_pairs;     /* pairs per merged launch quantum; 0 = auto */
+    uint32_t quantum_mcells;    /* DP cells per merged launch, in millions; 0 = 40,000 */
+    /* 0 (continuous admission): a job is admitted as soon as memory and a slot
+     * allow, and every admitted job gets an equal share of each merged launch.
+     * W > 0 (batch windows): a job is admitted at the first multiple of W
+     * microseconds (from server start) after its submission; windows are
+     * served in order, and the jobs of one window share the launches in
+     * proportion to their remaining cells, so they finish together. The
+     * next window's jobs are admitted while the previous one runs and fill
+     * its last launches. */
+    uint32_t batch_window_us;
 } msa_serve_config;
 
 typedef struct msa_job_stats {
@@ -294,11 +303,12 @@ typedef struct msa_job_stats {
     uint32_t launches;  /* merged launches this job's tiles were part of */
 } msa_job_stats;
 
-/* Starts a serving loop (continuous batching of all-pairs jobs) on a thread
- * owning its own context. No counterpart in the reference, which scores one
- * database per process run (src/museqa.cpp:223-236). Jobs are admitted in
- * arrival order while their device footprint fits the HBM budget; every
- * merged launch takes tasks round-robin from all admitted jobs. */
+/* Starts a serving loop (continuous batching of all-pairs jobs): an
+ * admission thread and a launch thread, each owning a context on the device.
+ * No counterpart in the reference, which scores one database per process run
+ * (src/museqa.cpp:223-236). Jobs are admitted in arrival order while their
+ * device footprint fits the HBM budget; every merged launch takes tasks from
+ * all admitted jobs, shared as batch_window_us says. */
 int msa_serve_start(const msa_serve_config *cfg, msa_server **out);
 /* Queues an all-pairs job (same inputs as msa_seqs_upload + table). */
 int msa_serve_submit(msa_server *srv, const uint8_t *units, const uint64_t *offs,

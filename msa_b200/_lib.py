@@ -70,7 +70,7 @@ class MsaNjStats(ctypes.Structure):
 
 class MsaServeConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_uint64), ("max_jobs", ctypes.c_uint32),
-                ("quantum_pairs", ctypes.c_uint32)]
+                ("quantum_mcells", ctypes.c_uint32), ("batch_window_us", ctypes.c_uint32)]
 
 
 class MsaJobStats(ctypes.Structure):

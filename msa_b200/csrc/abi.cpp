@@ -46,13 +46,12 @@ int cuda_error(msa_ctx *ctx, cudaError_t e, const char *what)
 static void free_store(SeqStore *st)
 {
     if(!st) return;
-    cudaFree(st->d_units);
-    cudaFree(st->d_off);
-    cudaFree(st->d_eff);
-    cudaFree(st->d_plen);
-    cudaFree(st->d_clean_sorted);
-    cudaFree(st->d_prof_off);
-    cudaFree(st->d_prof_lp);
+    void *bufs[] = {st->d_units, st->d_off, st->d_eff, st->d_plen, st->d_clean_sorted, st->d_prof_off, st->d_prof_lp};
+    for(void *p : bufs) {
+        if(!p) continue;
+        if(st->pooled) cudaFreeAsync(p, st->free_stream);
+        else cudaFree(p);
+    }
     delete st;
 }
 
@@ -184,7 +183,12 @@ int build_store(msa_ctx *ctx, const uint8_t *units, const uint64_t *offs, const 
         }
         st->prof_bytes = poff;
 
-        auto dmalloc = [&](void **p, size_t b) { return cudaMalloc(p, std::max<size_t>(b, 16)); };
+        st->pooled = ctx->pool != nullptr;
+        st->free_stream = ctx->stream;
+        auto dmalloc = [&](void **p, size_t b) {
+            return st->pooled ? cudaMallocFromPoolAsync(p, std::max<size_t>(b, 16), ctx->pool, ctx->stream)
+                              : cudaMalloc(p, std::max<size_t>(b, 16));
+        };
         cudaError_t e = cudaSuccess;
         if(!e) e = dmalloc((void **) &st->d_units, st->units_bytes);
         if(!e) e = dmalloc((void **) &st->d_off, n * sizeof(uint64_t));
@@ -219,6 +223,12 @@ int build_store(msa_ctx *ctx, const uint8_t *units, const uint64_t *offs, const 
 }
 
 void destroy_store(SeqStore *st) { free_store(st); }
+
+void destroy_store_async(SeqStore *st, cudaStream_t s)
+{
+    if(st && st->pooled) st->free_stream = s;
+    free_store(st);
+}
 
 }  // namespace msa
 

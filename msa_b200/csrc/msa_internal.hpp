@@ -71,6 +71,10 @@ struct SeqStore {
     uint64_t *d_prof_off = nullptr;
     uint32_t *d_prof_lp = nullptr;
     std::vector<std::string> names;   // record descriptions (msa_seqs_load_fasta)
+    // Device buffers came from the context's memory pool in stream order; they
+    // are returned in stream order on free_stream.
+    bool pooled = false;
+    cudaStream_t free_stream = nullptr;
 };
 
 // Growable device scratch buffer owned by a context.
@@ -100,6 +104,9 @@ struct msa_ctx {
     msa_nw_stats last{};
     msa_nj_stats nj_last{};
     msa::GraphCache *graphs = nullptr;
+    // When set, sequence stores are allocated from this pool on `stream`
+    // (no device-wide synchronisation on allocation or release).
+    cudaMemPool_t pool = nullptr;
     int tile_r = 0, tile_w = 0;   // persistent-kernel tile override (0 = autotuned)
 };
 
@@ -141,6 +148,8 @@ void release_graphs(msa_ctx *ctx);
 int build_store(msa_ctx *ctx, const uint8_t *units, const uint64_t *offs, const uint64_t *lens, uint32_t n,
                 SeqStore **out);
 void destroy_store(SeqStore *st);
+// Releases a pooled store's device memory in stream order on `s`.
+void destroy_store_async(SeqStore *st, cudaStream_t s);
 // Tile shape of the batched kernels for a store (committed autotuner table).
 struct Tiles { int R, W; };
 Tiles pick_tiles_for(const SeqStore *st);

@@ -1,20 +1,35 @@
 // Serving loop: continuous batching of all-pairs NW jobs on one device.
 //
-// Clients submit jobs (sequences + table) from any thread. A worker thread
-// owns a context and:
-//   * admits queued jobs in arrival order while their device footprint fits
-//     the HBM budget and a job slot is free: uploads the sequences, builds
-//     their score profiles and allocates the job's output triangle, all kept
-//     on the device until the job completes;
-//   * launches one merged persistent kernel per quantum, whose task list
-//     takes column groups round-robin from every admitted job, so work of a
-//     job that arrived while others were running shares the launch with them;
-//   * after each launch, finishes jobs whose last task ran (copies the scores
-//     out, frees the job's device memory) and admits more.
+// Clients submit jobs (sequences + table) from any thread. Two threads, each
+// with its own context and stream, serve them:
+//   * the admission thread takes queued jobs in arrival order while their
+//     device footprint fits the HBM budget and a job slot is free: uploads
+//     the sequences, builds their score profiles and allocates the job's
+//     output triangle, all kept on the device until the job completes;
+//   * the launch thread issues one merged persistent kernel per quantum,
+//     whose task list takes column groups from every admitted job, so work of
+//     a job that arrived while others were running shares the launch with
+//     them; two launches are kept in flight, and after each one the jobs whose
+//     last task ran are finished (scores copied out, device memory returned).
+// Job memory comes from a memory pool of the server in stream order, so
+// neither admission nor release waits for the launches in flight.
+//
+// Two policies share the quantum's cell budget among the admitted jobs:
+//   * continuous (batch_window_us = 0): every job gets an equal share, so a
+//     job's latency is about its own work times the number of jobs sharing the
+//     device;
+//   * batch windows (batch_window_us = W): a job submitted in window k (from
+//     server start) is admitted at the window's end, the windows are served in
+//     order (older windows take the budget first), and inside a window the
+//     budget is split in proportion to each job's remaining cells, so the jobs
+//     of a window advance together and finish in the same quantum. Latency is
+//     then close to the window's wait plus the window's work, whatever the
+//     job's own size.
 // Jobs containing sequences that need the reference's orientation (END units
 // inside a sequence, GAP units, a non-symmetric table) are scored at
-// admission by the single-job path on the same context.
+// admission by the single-job path on the admission context.
 #include <algorithm>
+#include <cmath>
 #include <atomic>
 #include <chrono>
 #include <condition_variable>
@@ -46,16 +61,20 @@ struct Job {
     double t_submit = 0, t_admit = 0, t_done = 0;
     uint64_t cells = 0;
     uint32_t launches = 0;
+    uint64_t window = 0;            // admission window index (batch windows)
     // device state while admitted
     SeqStore *st = nullptr;
-    DevBuf mem;
+    void *mem = nullptr;            // profiles, flags, table, output (pooled)
     int8_t *d_prof = nullptr;
     uint8_t *d_narrow = nullptr;
     int32_t *d_out = nullptr;
     uint64_t device_bytes = 0;
     std::vector<uint32_t> groups;   // column groups per rows pair
+    std::vector<uint8_t> narrow;    // 16-bit flag per rows pair (host copy)
+    const int8_t *d_ext = nullptr;  // extended table on the device
     uint32_t cur_k = 0, cur_g = 0;  // next task
     uint64_t total_tasks = 0, issued = 0, finished = 0;
+    uint64_t tcells_total = 0, tcells_issued = 0;   // estimated cells of all / issued tasks
     // result
     std::vector<int32_t> result;
     int status = MSA_OK;
@@ -66,10 +85,13 @@ struct Job {
 }  // namespace msa
 
 struct msa_server {
-    msa_ctx *ctx = nullptr;
-    std::thread worker;
+    msa_ctx *ctx = nullptr;   // launch thread
+    msa_ctx *adm = nullptr;   // admission thread
+    cudaMemPool_t pool = nullptr;
+    cudaStream_t adm_stream = nullptr;   // highest-priority stream of the admission context
+    std::thread worker, admitter;
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
+    std::condition_variable cv_work, cv_launch, cv_done;
     std::deque<msa::Job *> pending;
     std::vector<msa::Job *> admitted;
     std::map<uint64_t, msa::Job *> jobs;
@@ -77,6 +99,7 @@ struct msa_server {
     uint64_t next_id = 1;
     uint64_t budget = 0, used = 0;
     uint32_t max_jobs = 64, quantum = 0;
+    double window_ms = 0;   // admission window (0 = admit at once)
     double t0 = 0;
     // launch resources (worker thread only)
     msa::DevBuf bound, tasks, views, counter, tasks2, views2, counter2;
@@ -90,12 +113,28 @@ namespace {
 
 constexpr msa::Tiles kServeTiles{32, 8};
 
-// Admits a job. Sets *completed when the job was scored right away (the
-// reference-orientation path); the caller publishes completion under the lock.
+// Estimated cells of task (rows pair k, group g) of a job.
+static uint64_t task_cells(const Job *j, uint32_t k, uint32_t g)
+{
+    const SeqStore *st = j->st;
+    const uint32_t nclean = (uint32_t) st->clean_sorted.size();
+    const uint64_t e1 = st->eff[st->clean_sorted[2 * k]];
+    const uint32_t b0 = 2 * k + 1 + g * kServeTiles.W;
+    const uint32_t bn = std::min<uint32_t>(nclean, b0 + kServeTiles.W);
+    const uint64_t c0 = b0 < nclean ? st->eff[st->clean_sorted[b0]] : 0;
+    return 2 * e1 * c0 * (bn > b0 ? bn - b0 : 0);
+}
+
+// Admits a job on the admission context: uploads its sequences, table and
+// flags and allocates its output (the score profiles are left to
+// launch_job_profiles, so that the uploads of a batch of jobs do not queue
+// behind one another's kernels). Sets *completed when the job was scored
+// right away (the reference-orientation path); the caller publishes
+// completion under the lock.
 int admit_one(msa_server *srv, Job *j, bool *completed)
 {
     *completed = false;
-    msa_ctx *ctx = srv->ctx;
+    msa_ctx *ctx = srv->adm;
     j->t_admit = now_ms();
     int rc = build_store(ctx, j->units.data(), j->offs.data(), j->lens.data(), j->n, &j->st);
     if(rc) return rc;
@@ -114,8 +153,8 @@ int admit_one(msa_server *srv, Job *j, bool *completed)
     if(any_dirty || !symmetric || j->n < 2) {
         // Reference-orientation path on the same context, synchronously.
         if(j->n >= 2) {
-            DevBuf out;
-            cudaError_t e = out.ensure(npairs * 4);
+            void *out = nullptr;
+            cudaError_t e = cudaMallocFromPoolAsync(&out, npairs * 4, srv->pool, ctx->stream);
             if(e) return cuda_error(ctx, e, "job output");
             std::vector<uint8_t> saved_dirty = st->dirty;
             std::vector<uint32_t> saved_sorted = st->clean_sorted;
@@ -123,19 +162,19 @@ int admit_one(msa_server *srv, Job *j, bool *completed)
                 std::fill(st->dirty.begin(), st->dirty.end(), 1);
                 st->clean_sorted.clear();
             }
-            rc = nw_run(ctx, st, j->ext, MSA_NW_PERSISTENT, (int32_t *) out.ptr);
+            rc = nw_run(ctx, st, j->ext, MSA_NW_PERSISTENT, (int32_t *) out);
             st->dirty = saved_dirty;
             st->clean_sorted = saved_sorted;
             if(!rc) {
-                e = cudaMemcpyAsync(j->result.data(), out.ptr, npairs * 4, cudaMemcpyDeviceToHost, ctx->stream);
+                e = cudaMemcpyAsync(j->result.data(), out, npairs * 4, cudaMemcpyDeviceToHost, ctx->stream);
                 if(!e) e = cudaStreamSynchronize(ctx->stream);
                 if(e) rc = cuda_error(ctx, e, "job scores to host");
             }
             drop_plans_for_store(ctx, st->serial);
-            out.release();
+            cudaFreeAsync(out, ctx->stream);
             j->launches = 1;
         }
-        destroy_store(st);
+        destroy_store_async(st, ctx->stream);
         j->st = nullptr;
         j->t_done = now_ms();
         j->status = rc;
@@ -143,26 +182,37 @@ int admit_one(msa_server *srv, Job *j, bool *completed)
         return MSA_OK;   // completed at admission (status carries any error)
     }
     // Resident job: profiles, 16-bit flags, output triangle.
-    std::vector<uint8_t> narrow;
-    plan_rows_pairs(st, j->ext, kServeTiles, narrow, j->groups);
-    const uint32_t K = (uint32_t) narrow.size();
+    plan_rows_pairs(st, j->ext, kServeTiles, j->narrow, j->groups);
+    const uint32_t K = (uint32_t) j->narrow.size();
     j->total_tasks = 0;
-    for(uint32_t g : j->groups) j->total_tasks += g;
+    j->tcells_total = 0;
+    for(uint32_t k = 0; k < (uint32_t) j->groups.size(); ++k) {
+        j->total_tasks += j->groups[k];
+        for(uint32_t g = 0; g < j->groups[k]; ++g) j->tcells_total += task_cells(j, k, g);
+    }
     size_t off = 0;
     auto take = [&off](size_t b) { size_t o = off; off = round_up(off + b, 256); return o; };
     const size_t o_prof = take(st->prof_bytes + 64), o_ext = take(kAlpha * kAlpha), o_nar = take(K + 16),
                  o_out = take(npairs * 4);
-    cudaError_t e = j->mem.ensure(off);
-    if(e) return cuda_error(ctx, e, "job device memory");
-    char *base = (char *) j->mem.ptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&j->mem, off, srv->pool, ctx->stream);
+    if(e) { j->mem = nullptr; return cuda_error(ctx, e, "job device memory"); }
+    char *base = (char *) j->mem;
     j->d_prof = (int8_t *) (base + o_prof);
     j->d_narrow = (uint8_t *) (base + o_nar);
     j->d_out = (int32_t *) (base + o_out);
+    j->d_ext = (const int8_t *) (base + o_ext);
     e = cudaMemcpyAsync(base + o_ext, j->ext.score, kAlpha * kAlpha, cudaMemcpyHostToDevice, ctx->stream);
-    if(!e && K) e = cudaMemcpyAsync(j->d_narrow, narrow.data(), K, cudaMemcpyHostToDevice, ctx->stream);
-    if(!e) e = launch_profiles(st, (const int8_t *) (base + o_ext), j->d_prof, ctx->stream);
-    if(!e) e = cudaStreamSynchronize(ctx->stream);
+    if(!e && K) e = cudaMemcpyAsync(j->d_narrow, j->narrow.data(), K, cudaMemcpyHostToDevice, ctx->stream);
     if(e) return cuda_error(ctx, e, "job admission");
+    return MSA_OK;
+}
+
+// Score profiles of an admitted resident job, on the admission stream.
+int launch_job_profiles(msa_server *srv, Job *j)
+{
+    msa_ctx *ctx = srv->adm;
+    const cudaError_t e = launch_profiles(j->st, j->d_ext, j->d_prof, ctx->stream);
+    if(e) return cuda_error(ctx, e, "job profiles");
     ctx->launches++;
     return MSA_OK;
 }
@@ -177,10 +227,12 @@ uint64_t estimate_bytes(const Job *j)
     return units + prof + (uint64_t) j->n * (j->n > 0 ? j->n - 1 : 0) * 2 + (uint64_t) j->n * 40 + 4096;
 }
 
-void release_job_device(Job *j)
+// Returns a job's device memory to the pool in stream order on `s` (the
+// job's last launch has completed, or it never ran).
+void release_job_device(Job *j, cudaStream_t s)
 {
-    if(j->st) { destroy_store(j->st); j->st = nullptr; }
-    j->mem.release();
+    if(j->st) { destroy_store_async(j->st, s); j->st = nullptr; }
+    if(j->mem) { cudaFreeAsync(j->mem, s); j->mem = nullptr; }
 }
 
 // One launch in flight: its completion event and the tasks it took per job.
@@ -215,26 +267,91 @@ struct InFlight {
     }
 };
 
-// Estimated cells of task (rows pair k, group g) of a job.
-static uint64_t task_cells(const Job *j, uint32_t k, uint32_t g)
+// Admission thread: takes queued jobs in arrival order (at their window's
+// end under batch windows) while the HBM budget and the job slots allow, and
+// hands them to the launch thread. All jobs eligible at once are admitted as
+// one batch: their uploads first, then their profile kernels, then a single
+// wait. The admission stream has the device's highest priority, so these
+// kernels take SMs at the next boundary of the merged launches.
+void admission_loop(msa_server *srv)
 {
-    const SeqStore *st = j->st;
-    const uint32_t nclean = (uint32_t) st->clean_sorted.size();
-    const uint64_t e1 = st->eff[st->clean_sorted[2 * k]];
-    const uint32_t b0 = 2 * k + 1 + g * kServeTiles.W;
-    const uint32_t bn = std::min<uint32_t>(nclean, b0 + kServeTiles.W);
-    const uint64_t c0 = b0 < nclean ? st->eff[st->clean_sorted[b0]] : 0;
-    return 2 * e1 * c0 * (bn > b0 ? bn - b0 : 0);
+    msa_ctx *ctx = srv->adm;
+    cudaSetDevice(ctx->device);
+    for(;;) {
+        std::vector<Job *> batch;
+        {
+            std::unique_lock<std::mutex> lk(srv->mu);
+            for(;;) {
+                if(srv->stop) return;
+                double wait_ms = 20.0;
+                const double now = now_ms();
+                while(!srv->pending.empty() && srv->admitted.size() + batch.size() < srv->max_jobs) {
+                    Job *f = srv->pending.front();
+                    const double gate = srv->window_ms > 0 ? srv->t0 + (double) f->window * srv->window_ms : 0.0;
+                    if(now < gate) {
+                        wait_ms = std::max(0.05, std::min(wait_ms, gate - now));
+                        break;
+                    }
+                    const uint64_t need = estimate_bytes(f);
+                    // A job larger than the whole budget is admitted alone.
+                    if(srv->used + need > srv->budget && !(srv->admitted.empty() && batch.empty())) break;
+                    srv->pending.pop_front();
+                    f->device_bytes = need;
+                    srv->used += need;
+                    batch.push_back(f);
+                }
+                if(!batch.empty()) break;
+                srv->cv_work.wait_for(lk, std::chrono::microseconds((long long) (wait_ms * 1000)));
+            }
+        }
+        std::vector<int> status(batch.size(), MSA_OK);
+        std::vector<char> completed(batch.size(), 0);
+        for(size_t i = 0; i < batch.size(); ++i) {
+            bool done = false;
+            status[i] = admit_one(srv, batch[i], &done);
+            completed[i] = done;
+        }
+        for(size_t i = 0; i < batch.size(); ++i)
+            if(!status[i] && !completed[i]) status[i] = launch_job_profiles(srv, batch[i]);
+        const cudaError_t e = cudaStreamSynchronize(ctx->stream);
+        if(e) {
+            const int rc = cuda_error(ctx, e, "job admission");
+            for(size_t i = 0; i < batch.size(); ++i) if(!completed[i] && !status[i]) status[i] = rc;
+        }
+        for(size_t i = 0; i < batch.size(); ++i) {
+            Job *j = batch[i];
+            if(status[i] || completed[i]) {
+                if(status[i]) { j->status = status[i]; j->t_done = now_ms(); }
+                release_job_device(j, ctx->stream);
+            }
+        }
+        std::lock_guard<std::mutex> lk(srv->mu);
+        bool any = false;
+        for(size_t i = 0; i < batch.size(); ++i) {
+            Job *j = batch[i];
+            if(status[i] || completed[i]) {
+                srv->used -= j->device_bytes;
+                j->done = true;
+            } else {
+                srv->admitted.push_back(j);
+                any = true;
+            }
+        }
+        srv->cv_done.notify_all();
+        if(any) srv->cv_launch.notify_one();
+    }
 }
 
+// Launch thread: merged launches over the admitted jobs, two in flight.
 void worker_loop(msa_server *srv)
 {
     msa_ctx *ctx = srv->ctx;
     cudaSetDevice(ctx->device);
-    cudaStream_t compute = ctx->own_stream, upload = nullptr;
-    cudaStreamCreateWithFlags(&upload, cudaStreamNonBlocking);
-    cudaEvent_t uploaded = nullptr;
-    cudaEventCreateWithFlags(&uploaded, cudaEventDisableTiming);
+    cudaStream_t compute = ctx->own_stream, drain = nullptr;
+    cudaStreamCreateWithFlags(&drain, cudaStreamNonBlocking);
+    // Job memory goes back to the pool on the admission stream, where the next
+    // admissions reuse it without waiting for this thread's launches.
+    cudaStream_t release_stream = srv->adm->stream;
     InFlight slots[2];
     for(auto &f : slots) cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming);
     int cur = 0;
@@ -254,12 +371,12 @@ void worker_loop(msa_server *srv)
             if(j->finished >= j->total_tasks && !j->done) {
                 if(!e && j->status == MSA_OK) {
                     const uint64_t npairs = (uint64_t) j->n * (j->n - 1) / 2;
-                    cudaError_t e2 = cudaMemcpyAsync(j->result.data(), j->d_out, npairs * 4, cudaMemcpyDeviceToHost, upload);
-                    if(!e2) e2 = cudaStreamSynchronize(upload);
+                    cudaError_t e2 = cudaMemcpyAsync(j->result.data(), j->d_out, npairs * 4, cudaMemcpyDeviceToHost, drain);
+                    if(!e2) e2 = cudaStreamSynchronize(drain);
                     if(e2) j->status = cuda_error(ctx, e2, "job scores to host");
                 }
                 j->t_done = now_ms();
-                release_job_device(j);
+                release_job_device(j, release_stream);
                 finished.push_back(j);
             }
         }
@@ -275,70 +392,59 @@ void worker_loop(msa_server *srv)
                 j->done = true;
             }
             srv->cv_done.notify_all();
+            srv->cv_work.notify_all();   // memory and job slots are free again
         }
     };
 
+    const uint64_t budget_cells = srv->quantum ? (uint64_t) srv->quantum * 1000000ull : 40000000000ull;
     for(;;) {
-        // 1. Admission on the upload stream (does not wait for launches in flight).
-        std::vector<Job *> to_admit;
-        bool idle = false;
+        // 1. Retire the launch that used this slot two rounds ago.
+        retire(slots[cur]);
+
+        // 2. The admitted jobs with tasks left (in admission order).
+        std::vector<Job *> active;
         {
             std::unique_lock<std::mutex> lk(srv->mu);
             if(srv->stop) break;
-            while(!srv->pending.empty() && srv->admitted.size() + to_admit.size() < srv->max_jobs) {
-                Job *j = srv->pending.front();
-                const uint64_t need = estimate_bytes(j);
-                if(srv->used + need > srv->budget && !(srv->admitted.empty() && to_admit.empty())) break;
-                srv->pending.pop_front();
-                j->device_bytes = need;
-                srv->used += need;
-                to_admit.push_back(j);
-            }
-            idle = to_admit.empty() && srv->admitted.empty() && !slots[0].busy && !slots[1].busy;
-            if(idle) {
-                srv->cv_work.wait_for(lk, std::chrono::milliseconds(20));
+            for(Job *j : srv->admitted) if(j->issued < j->total_tasks) active.push_back(j);
+            if(active.empty() && !slots[cur ^ 1].busy) {
+                srv->cv_launch.wait_for(lk, std::chrono::milliseconds(20));
                 continue;
             }
-        }
-        if(!to_admit.empty()) {
-            ctx->stream = upload;
-            for(Job *j : to_admit) {
-                bool completed = false;
-                const int rc = admit_one(srv, j, &completed);
-                if(rc || completed) {
-                    if(rc) { j->status = rc; j->t_done = now_ms(); }
-                    release_job_device(j);
-                }
-                std::lock_guard<std::mutex> lk(srv->mu);
-                if(rc || completed) {
-                    srv->used -= j->device_bytes;
-                    j->done = true;
-                    srv->cv_done.notify_all();
-                } else {
-                    srv->admitted.push_back(j);
-                }
-            }
-            ctx->stream = compute;
-            cudaEventRecord(uploaded, upload);
-            cudaStreamWaitEvent(compute, uploaded, 0);
-        }
-
-        // 2. Retire the launch that used this slot two rounds ago.
-        retire(slots[cur]);
-
-        std::vector<Job *> active;
-        {
-            std::lock_guard<std::mutex> lk(srv->mu);
-            for(Job *j : srv->admitted) if(j->issued < j->total_tasks) active.push_back(j);
         }
         if(active.empty()) {
             retire(slots[cur ^ 1]);
             continue;
         }
 
-        // 3. Build one merged launch: an equal share of the cell budget per job,
-        // tasks taken round-robin in each job's cost order, then sorted longest
-        // first so the launch's tail holds its smallest tasks.
+        // 3. Each job's cell quota in this launch.
+        std::vector<uint64_t> quota(active.size(), 0);
+        if(srv->window_ms > 0) {
+            // Windows in order; the last window reached splits what is left
+            // in proportion to its jobs' remaining cells.
+            uint64_t left = budget_cells;
+            for(size_t a = 0; a < active.size() && left > 0;) {
+                size_t b = a;
+                uint64_t rem = 0;
+                while(b < active.size() && active[b]->window == active[a]->window) {
+                    rem += active[b]->tcells_total - active[b]->tcells_issued;
+                    ++b;
+                }
+                for(size_t i = a; i < b; ++i) {
+                    const uint64_t r = active[i]->tcells_total - active[i]->tcells_issued;
+                    quota[i] = rem <= left ? ~0ull
+                                           : std::max<uint64_t>((uint64_t) ((unsigned __int128) left * r / std::max<uint64_t>(rem, 1)), 1);
+                }
+                left = rem <= left ? left - rem : 0;
+                a = b;
+            }
+        } else {
+            std::fill(quota.begin(), quota.end(), std::max<uint64_t>(budget_cells / active.size(), 1));
+        }
+
+        // 4. One merged launch: tasks taken in each job's cost order up to its
+        // quota, then sorted longest first so the launch's tail holds its
+        // smallest tasks.
         uint64_t max_cols = 1;
         for(Job *j : active) for(uint32_t i = 0; i < j->n; ++i) max_cols = std::max<uint64_t>(max_cols, j->st->plen[i]);
         const uint64_t stride = round_up(max_cols + 160, 32);
@@ -348,8 +454,6 @@ void worker_loop(msa_server *srv)
             if(srv->bound.ensure(srv->grid * kServeTiles.W * std::max<uint64_t>(stride, 2048 + 160) * 4)) break;
             srv->bound_stride = std::max<uint64_t>(stride, 2048 + 160);
         }
-        const uint64_t budget_cells = srv->quantum ? (uint64_t) srv->quantum * 1000000ull : 40000000000ull;
-        const uint64_t share = std::max<uint64_t>(budget_cells / active.size(), 1);
         struct T { uint32_t slot, k, g; uint64_t cost; };
         std::vector<T> tasks;
         InFlight &f = slots[cur];
@@ -359,7 +463,7 @@ void worker_loop(msa_server *srv)
             Job *j = active[sl];
             fill_job_view(srv->h_views.data() + sl * vb, j->st, j->d_prof, j->d_narrow, j->d_out, j->ext.penalty);
             uint64_t taken = 0, cells = 0;
-            while(j->issued + taken < j->total_tasks && cells < share) {
+            while(j->issued + taken < j->total_tasks && cells < quota[sl]) {
                 while(j->cur_k < j->groups.size() && j->cur_g >= j->groups[j->cur_k]) { ++j->cur_k; j->cur_g = 0; }
                 const uint64_t c = task_cells(j, j->cur_k, j->cur_g);
                 tasks.push_back({(uint32_t) sl, j->cur_k, j->cur_g, c});
@@ -368,6 +472,7 @@ void worker_loop(msa_server *srv)
                 ++taken;
             }
             j->issued += taken;
+            j->tcells_issued += cells;
             if(taken) { f.work.push_back({j, taken}); ++j->launches; }
         }
         std::stable_sort(tasks.begin(), tasks.end(), [](const T &a, const T &b) { return a.cost > b.cost; });
@@ -405,15 +510,7 @@ void worker_loop(msa_server *srv)
     retire(slots[0]);
     retire(slots[1]);
     for(auto &f : slots) { cudaEventDestroy(f.done); f.release(); }
-    cudaEventDestroy(uploaded);
-    cudaStreamDestroy(upload);
-    // Stopping: fail what is still queued or admitted.
-    std::lock_guard<std::mutex> lk(srv->mu);
-    for(Job *j : srv->pending) { j->status = MSA_ERR_QUEUE; j->done = true; }
-    srv->pending.clear();
-    for(Job *j : srv->admitted) { release_job_device(j); j->status = MSA_ERR_QUEUE; j->done = true; }
-    srv->admitted.clear();
-    srv->cv_done.notify_all();
+    cudaStreamDestroy(drain);
 }
 
 }  // namespace
@@ -431,20 +528,64 @@ int msa_serve_start(const msa_serve_config *cfg, msa_server **out)
     try {
         srv = new msa_server;
         int rc = msa_create(cfg->device, &srv->ctx);
-        if(rc) { delete srv; return rc; }
+        if(!rc) rc = msa_create(cfg->device, &srv->adm);
+        if(!rc) {
+            cudaMemPoolProps props{};
+            props.allocType = cudaMemAllocationTypePinned;
+            props.location.type = cudaMemLocationTypeDevice;
+            props.location.id = cfg->device;
+            if(cudaMemPoolCreate(&srv->pool, &props) != cudaSuccess) {
+                cudaGetLastError();
+                srv->pool = nullptr;
+                rc = MSA_ERR_CUDA;
+            } else {
+                // Keep released memory in the pool for the next jobs, and never
+                // let an allocation on one stream wait for another stream's work.
+                uint64_t keep = ~0ull;
+                int no = 0;
+                cudaMemPoolSetAttribute(srv->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+                cudaMemPoolSetAttribute(srv->pool, cudaMemPoolReuseAllowInternalDependencies, &no);
+                srv->adm->pool = srv->pool;
+                int least = 0, greatest = 0;
+                cudaDeviceGetStreamPriorityRange(&least, &greatest);
+                if(cudaStreamCreateWithPriority(&srv->adm_stream, cudaStreamNonBlocking, greatest) == cudaSuccess)
+                    srv->adm->stream = srv->adm_stream;
+                else
+                    cudaGetLastError();
+            }
+        }
+        if(rc) {
+            if(srv->adm) msa_destroy(srv->adm);
+            if(srv->ctx) msa_destroy(srv->ctx);
+            delete srv;
+            return rc;
+        }
         size_t free_b = 0, total_b = 0;
         cudaSetDevice(cfg->device);
         if(cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { cudaGetLastError(); free_b = 0; }
         srv->budget = cfg->hbm_budget_bytes ? cfg->hbm_budget_bytes : (uint64_t) (0.8 * (double) free_b);
         srv->max_jobs = cfg->max_jobs ? cfg->max_jobs : 64;
-        srv->quantum = cfg->quantum_pairs;
+        srv->quantum = cfg->quantum_mcells;
+        srv->window_ms = cfg->batch_window_us / 1000.0;
         srv->t0 = now_ms();
         srv->worker = std::thread(worker_loop, srv);
+        srv->admitter = std::thread(admission_loop, srv);
         *out = srv;
         return MSA_OK;
     } catch(...) {
         if(srv) {
+            {
+                std::lock_guard<std::mutex> lk(srv->mu);
+                srv->stop = true;
+            }
+            srv->cv_work.notify_all();
+            srv->cv_launch.notify_all();
+            if(srv->worker.joinable()) srv->worker.join();
+            if(srv->admitter.joinable()) srv->admitter.join();
+            if(srv->adm) msa_destroy(srv->adm);
+            if(srv->adm_stream) cudaStreamDestroy(srv->adm_stream);
             if(srv->ctx) msa_destroy(srv->ctx);
+            if(srv->pool) cudaMemPoolDestroy(srv->pool);
             delete srv;
         }
         return MSA_ERR_NOMEM;
@@ -479,6 +620,7 @@ int msa_serve_submit(msa_server *srv, const uint8_t *units, const uint64_t *offs
         if(srv->stop) { delete j; return MSA_ERR_QUEUE; }
         j->id = srv->next_id++;
         j->t_submit = now_ms();
+        if(srv->window_ms > 0) j->window = (uint64_t) std::ceil((j->t_submit - srv->t0) / srv->window_ms);
         srv->jobs[j->id] = j;
         srv->pending.push_back(j);
         *job_id = j->id;
@@ -521,14 +663,23 @@ int msa_serve_stop(msa_server *srv)
         std::lock_guard<std::mutex> lk(srv->mu);
         srv->stop = true;
         srv->cv_work.notify_all();
+        srv->cv_launch.notify_all();
     }
+    if(srv->admitter.joinable()) srv->admitter.join();
     if(srv->worker.joinable()) srv->worker.join();
+    cudaSetDevice(srv->ctx->device);
     {
+        // Fail what is still queued or admitted.
         std::lock_guard<std::mutex> lk(srv->mu);
+        for(Job *j : srv->pending) { j->status = MSA_ERR_QUEUE; j->done = true; }
+        srv->pending.clear();
+        for(Job *j : srv->admitted) { release_job_device(j, srv->adm->stream); j->status = MSA_ERR_QUEUE; j->done = true; }
+        srv->admitted.clear();
+        srv->cv_done.notify_all();
         for(auto &kv : srv->jobs) delete kv.second;
         srv->jobs.clear();
     }
-    cudaSetDevice(srv->ctx->device);
+    cudaStreamSynchronize(srv->adm->stream);
     srv->bound.release();
     srv->tasks.release();
     srv->views.release();
@@ -536,7 +687,10 @@ int msa_serve_stop(msa_server *srv)
     srv->tasks2.release();
     srv->views2.release();
     srv->counter2.release();
+    msa_destroy(srv->adm);
+    if(srv->adm_stream) cudaStreamDestroy(srv->adm_stream);
     msa_destroy(srv->ctx);
+    if(srv->pool) cudaMemPoolDestroy(srv->pool);
     delete srv;
     return MSA_OK;
 }

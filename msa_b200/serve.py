@@ -20,8 +20,10 @@ from .pairwise import ScoringTable
 
 
 class Server:
-    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, max_jobs: int = 0, quantum: int = 0):
-        cfg = MsaServeConfig(device, hbm_budget_bytes, max_jobs, quantum)
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, max_jobs: int = 0, quantum_mcells: int = 0,
+                 batch_window_ms: float = 0.0):
+        """batch_window_ms > 0 admits jobs at window boundaries (msa_serve_config.batch_window_us)."""
+        cfg = MsaServeConfig(device, hbm_budget_bytes, max_jobs, quantum_mcells, int(round(batch_window_ms * 1000)))
         h = ctypes.c_void_p()
         check(lib().msa_serve_start(ctypes.byref(cfg), ctypes.byref(h)))
         self.handle = h

@@ -96,3 +96,22 @@ def test_wait_with_timeout_and_unknown_job(gpu):
         if rc == _lib.MSA_ERR_DEVICE_TIMEOUT:
             srv.wait(jid)
         assert _lib.lib().msa_serve_wait(srv.handle, 987654, 0, None, None) == _lib.MSA_ERR_QUEUE
+
+
+def test_windowed_admission_starts_jobs_on_window_boundaries(gpu):
+    """batch_window_ms > 0: a job is admitted at the first window boundary
+    after its submission (counted from server start), and its scores are
+    still those of the job alone."""
+    jobs = [W.c5_job(4000 + k) for k in range(5)]
+    for wl in jobs:
+        wl.seqs = wl.seqs[:60]
+    window = 30.0
+    with Server(device=0, batch_window_ms=window) as srv:
+        ids = []
+        for wl in jobs:
+            ids.append(srv.submit_workload(wl))
+        results = [srv.wait(i) for i in ids]
+    for wl, (scores, stats) in zip(jobs, results):
+        assert np.array_equal(scores, _alone(wl))
+        boundary = np.ceil(stats["submit_ms"] / window) * window
+        assert stats["admit_ms"] >= boundary - 1e-3
