@@ -231,7 +231,18 @@ def nj_leg(lib, ctx, steps: int = 3, cpu: bool = True) -> dict:
 # ---------------------------------------------------------------- GPU arm
 
 PROBE_OPS = ["iadd", "imnmx", "viaddmax_s32", "vimax3_s32", "vadd2", "viaddmax_s16x2", "vimax3_s16x2",
-             "viaddmax_u16x2", "vimax3_u16x2", "vmaxu2", "prmt", "cell_s32", "cell_s16x2", "cell_u16x2_biased"]
+             "viaddmax_u16x2", "vimax3_u16x2", "vmaxu2", "prmt", "cell_s32", "cell_s16x2", "cell_u16x2_biased",
+             "cell_u16x2_gapfree", "lds128_bytes"]
+
+
+def probe_rate(ctx, op: int, iters: int = 2048) -> float:
+    """Lane-ops (op 15: shared-memory bytes) per SM per clock of one probe form."""
+    import ctypes
+
+    from msa_b200 import _lib
+    p = _lib.MsaOpProbe()
+    _lib.check(_lib.lib().msa_probe_op(ctx.handle, op, iters, ctypes.byref(p)), ctx.handle)
+    return float(p.ops_per_clk_sm)
 
 
 def probe_ops(iters: int = 2048) -> dict:
@@ -276,10 +287,14 @@ def serve_bench(args):
     sat_gcups = total_cells / sat_s / 1e9
 
     rate = args.load * (sat_gcups * 1e9) / mean_cells          # jobs per second
-    rng = np.random.Generator(np.random.PCG64(5))
-    arrivals = np.cumsum(rng.exponential(1.0 / rate, len(jobs)))
 
-    def run_server(window_ms=0.0):
+    def arrival_times(seed):
+        rng = np.random.Generator(np.random.PCG64(seed))
+        return np.cumsum(rng.exponential(1.0 / rate, len(jobs)))
+
+    arrivals = arrival_times(5)
+
+    def run_server(window_ms=0.0, arrivals=arrivals):
         stats = [None] * len(jobs)
         with Server(device=0, batch_window_ms=window_ms) as srv:
             ids = [None] * len(jobs)
@@ -306,6 +321,16 @@ def serve_bench(args):
         return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
                 "p99_over_p50": float(np.percentile(lat, 99) / np.percentile(lat, 50)), "aggregate_gcups": agg,
                 "mean_launches_per_job": float(np.mean([s["launches"] for s in stats]))}
+
+    if args.sweep_windows:
+        # Window x arrival-seed sweep at the same offered load (no plain leg).
+        seeds = [int(x) for x in args.arrival_seeds.split(",")]
+        for w in [float(x) for x in args.sweep_windows.split(",")]:
+            for seed in seeds:
+                lat, agg, st = run_server(w, arrival_times(seed))
+                print(json.dumps({"window_ms": w, "arrival_seed": seed, **summary(lat, agg, st),
+                                  "saturated_gcups": sat_gcups, "arrival_rate_per_s": rate}), flush=True)
+        return None
 
     continuous = summary(*run_server())
     windowed = summary(*run_server(args.window_ms)) if args.window_ms > 0 else None
@@ -480,7 +505,10 @@ def main():
     ap.add_argument("--serve", action="store_true", help="serving loop: Poisson arrivals of c5 jobs")
     ap.add_argument("--jobs", type=int, default=400)
     ap.add_argument("--load", type=float, default=0.8, help="offered load as a fraction of saturated throughput")
-    ap.add_argument("--window-ms", type=float, default=40.0,
+    ap.add_argument("--sweep-windows", default="",
+                    help="with --serve: comma-separated batch windows (ms, 0 = continuous) to sweep instead")
+    ap.add_argument("--arrival-seeds", default="5,6,7", help="with --sweep-windows: Poisson arrival seeds")
+    ap.add_argument("--window-ms", type=float, default=60.0,
                     help="with --serve: batch window of the headline serving run (0: continuous admission only)")
     args = ap.parse_args()
     if args.probe:
@@ -609,11 +637,18 @@ def main():
     if rank == 0:
         props = torch.cuda.get_device_properties(local)
         sm_mhz = clocks.get("sm_mhz") or 1965.0
-        # Integer-issue roofline: max-plus needs two max operations per cell and
-        # every max form (DPX included) issues on the ALU pipe, 64 lanes/clk/SM
-        # (measured by `bench.py --probe`): 32 cells/clk/SM in 32-bit lanes,
-        # 64 in 16x2 lanes.
-        peak = props.multi_processor_count * 64 * sm_mhz * 1e6 / 2 / 1e9
+        nsm = props.multi_processor_count
+        # Ceilings of the batched kernel's cell, from rates measured here per SM
+        # clock (msa_probe_op): each 16x2 lane-op of the cell form updates two
+        # cells, and every cell reads one 16-bit profile half (2 bytes) from
+        # shared memory. The shared-memory one is the lowest: the roofline.
+        lds = probe_rate(ctx, 15)
+        cell_ops = probe_rate(ctx, 14)
+        smem_peak = nsm * (lds / 2.0) * sm_mhz * 1e6 / 1e9
+        cell_peak = nsm * (2.0 * cell_ops) * sm_mhz * 1e6 / 1e9
+        # The four-op int32 issue figure (two max operations per cell on the ALU
+        # pipe, 64 lanes/clk/SM): 32 cells/clk/SM.
+        peak = nsm * 64 * sm_mhz * 1e6 / 2 / 1e9
         traffic = None
         tp = ROOT / "profiles" / "nw_traffic.json"
         if tp.exists():
@@ -637,13 +672,16 @@ def main():
                     "h2d_bytes_per_step": int(flat.nbytes + offs.nbytes + lens.nbytes),
                     "d2h_bytes_per_step": int(npairs * 4), "scores_match": e2e_ok},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "int32-issue", "achieved": kernel_gcups, "peak": peak, "unit": "GCUPS",
-                         "frac": kernel_gcups / peak, "frac_x2": kernel_gcups / (2 * peak), "traffic": traffic,
-                         "ceilings_gcups": {"int32_lanes_alu": peak, "int16x2_lanes_alu": 2 * peak,
-                                            "int16x2_lanes_alu_plus_fma": 8 * peak / 3},
-                         "peak_basis": f"{props.multi_processor_count} SM x 64 ALU lanes/clk x {sm_mhz:.0f} MHz "
-                                       f"(median sampled) / 2 max-ops per cell (int32 lanes); frac_x2 is against "
-                                       f"the 16x2-lane ceiling, twice that"},
+            "roofline": {"bound": "smem", "achieved": kernel_gcups, "peak": smem_peak, "unit": "GCUPS",
+                         "frac": kernel_gcups / smem_peak, "traffic": traffic,
+                         "frac_int32_issue": kernel_gcups / peak,
+                         "ceilings_gcups": {"smem_profile_reads": smem_peak, "cell_ops_16x2": cell_peak,
+                                            "int32_issue_4ops_per_cell": peak},
+                         "measured_per_sm_clk": {"lds_bytes": lds, "cell_16x2_lane_ops": cell_ops},
+                         "peak_basis": f"{nsm} SM x {lds:.1f} shared-memory bytes/clk (measured, ld.shared.v4) / "
+                                       f"2 bytes of profile per cell x {sm_mhz:.0f} MHz (median sampled); "
+                                       f"frac_int32_issue is against {nsm} SM x 64 ALU lanes/clk / 2 max-ops "
+                                       f"per cell"},
             "clocks": clocks,
             "cpu_baseline": cpu,
         }

@@ -328,7 +328,9 @@ int msa_serve_stop(msa_server *srv);
  * it measures the INT32 issue roofline the NW kernels are reported against).
  * op: 0 IADD, 1 IMNMX, 2 viaddmax_s32, 3 vimax3_s32, 4 vadd2, 5 viaddmax_s16x2,
  * 6 vimax3_s16x2, 7 viaddmax_u16x2, 8 vimax3_u16x2, 9 vmaxu2, 10 PRMT,
- * 11 the 32-bit NW cell, 12 the signed 16x2 NW cell, 13 the biased 16x2 cell.
+ * 11 the 32-bit NW cell, 12 the signed 16x2 NW cell, 13 the biased 16x2 cell,
+ * 14 the 16x2 cell on the gap-free state (vadd2 + vimax3_u16x2),
+ * 15 shared-memory ld.shared.v4 bandwidth (ops_per_clk_sm = bytes per SM per clock).
  */
 typedef struct msa_op_probe {
     double ops_per_clk_sm;  /* lane-operations per SM per SM clock */

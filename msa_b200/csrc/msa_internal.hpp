@@ -42,6 +42,8 @@ struct ExtTable {
     int32_t max_abs;   // max |score| over valid entries (END row/column excluded)
     int32_t max_pos;   // largest score
     int32_t max_neg;   // largest magnitude of a negative score
+    int32_t letter_pos;   // largest score among letter units (0..23), the only
+    int32_t letter_neg;   // units of clean sequences; and its largest negative magnitude
 };
 int make_ext_table(const msa_table *t, ExtTable *out, std::string *err);
 

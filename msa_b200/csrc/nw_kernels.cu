@@ -73,26 +73,22 @@ struct Wide {
 };
 
 // Two cells per 32-bit lane (16-bit halves: the two rows sequences of a rows
-// pair). The lane state is not H but S = H - g + 0x8000 per half, in which a
-// cell is S = max(S_left - g, S_up - g, S_diag + s), computed in one of two
-// forms:
-//   two maxes:       max(S_up - g, max(S_left - g, S_diag + s))
-//                    two viaddmax_u16x2 (ALU) and a vadd2 (FMA); one dependent
-//                    operation on the chain down a lane's rows;
-//   three-way max:   vimax3_u16x2(S_left, S_up, S_diag + (s + g)) - g
-//                    one ALU max, a vadd2 and a 32-bit subtract either integer
-//                    pipe may take; two dependent operations on the chain.
-// Even rows of a lane take the first form and odd rows the second (the staged
-// words hold s or s + g accordingly), which spreads the work over both integer
-// pipes while keeping the row chain short. The 0x8000 bias keeps every half at
-// or above g under the 16-bit bound narrow_ok proves, so the 32-bit subtract
-// never borrows across halves, the unsigned maxes order biased values exactly,
-// and S - g never wraps.
+// pair). The lane state is not H but T(i,j) = H(i,j) + g*(i + j), unsigned per
+// half. The gap terms cancel out of the recurrence:
+//   T = max(T_left, T_up, T_diag + (s + 2g)),
+// one vadd2 (FMA pipe, off the row chain) and one vimax3_u16x2 (ALU pipe, the
+// only operation on the chain down a lane's rows); the staged profile words
+// hold s + 2g. Row 0 and column 0 of T are 0. Over every path T = the sum of
+// (s + 2g) over its matched cells, so 0 <= T(i,j) <= min(i,j)*(smax + 2g) when
+// smin + 2g >= 0 (narrow_ok checks both), and the diagonal candidate never
+// exceeds the cell it competes for: no half leaves [0, 0xffff]. Every operation
+// stays inside its 16-bit half, so rows past a sequence's end (padding, or the
+// shorter sequence of the pair) hold values that never reach a scored cell.
 struct Narrow {
     using W = uint32_t;
-    __device__ static __forceinline__ W state(int32_t h, int32_t g) { return ((uint32_t) (h - g + 0x8000) & 0xffffu) * 0x10001u; }
-    __device__ static __forceinline__ int32_t lo(W w, int32_t g) { return (int32_t) (w & 0xffffu) - 0x8000 + g; }
-    __device__ static __forceinline__ int32_t hi(W w, int32_t g) { return (int32_t) (w >> 16) - 0x8000 + g; }
+    // H(rows, cols) from the low or high half of T(rows, cols).
+    __device__ static __forceinline__ int32_t lo(W w, int32_t g, int rows, int cols) { return (int32_t) (w & 0xffffu) - g * (rows + cols); }
+    __device__ static __forceinline__ int32_t hi(W w, int32_t g, int rows, int cols) { return (int32_t) (w >> 16) - g * (rows + cols); }
     __device__ static __forceinline__ W splat(int32_t v) { return dup16(v); }
 };
 
@@ -421,14 +417,13 @@ namespace dev {
 // Stages strip rows [i0, i0 + 32R) as 32-bit profile words in shared memory,
 // laid out [code][plane of 4 rows][lane][4 words] so that one 16-byte load per
 // lane and plane is bank-conflict free for any codes the lanes hold.
-// Narrow: word = (s(X1_i, b), s(X2_i, b)) as int16x2, plus g in both halves on
-// odd rows of a lane; rows of X2 past its profile (lp2) score 0. Wide: word =
-// s(X1_i, b) as int32.
+// Narrow: word = (s(X1_i, b) + 2g, s(X2_i, b) + 2g) as 16x2 (see Narrow);
+// rows of X2 past its profile (lp2) score 0. Wide: word = s(X1_i, b) as int32.
 template <int R, bool kNarrow>
 __device__ __forceinline__ void stage_words(uint32_t *sprof, const int8_t *__restrict__ g1, uint32_t lp1,
                                             const int8_t *__restrict__ g2, uint32_t lp2, int i0, int32_t gap = 0)
 {
-    const uint32_t gg = ((uint32_t) gap & 0xffffu) * 0x10001u;
+    const uint32_t gg = ((uint32_t) (2 * gap) & 0xffffu) * 0x10001u;
     constexpr int SH = 32 * R;
     constexpr int G = SH / 4;        // 4-row groups per code row
     constexpr int PL = R / 4;        // planes per lane
@@ -440,11 +435,9 @@ __device__ __forceinline__ void stage_words(uint32_t *sprof, const int8_t *__res
         if constexpr(kNarrow) {
             uint32_t vb = 0;
             if((uint32_t) (i0 + 4 * rg) < lp2) vb = __ldg(reinterpret_cast<const uint32_t *>(g2 + (size_t) b * lp2 + i0) + rg);
-            // Even rows of a lane take the two-max form (score s), odd rows
-            // the three-way-max form (score s + g); see Narrow.
-            o.x = sbyte2<0>(va, vb);
+            o.x = __vadd2(sbyte2<0>(va, vb), gg);
             o.y = __vadd2(sbyte2<1>(va, vb), gg);
-            o.z = sbyte2<2>(va, vb);
+            o.z = __vadd2(sbyte2<2>(va, vb), gg);
             o.w = __vadd2(sbyte2<3>(va, vb), gg);
         } else {
             o.x = (uint32_t) sbyte<0>(va);
@@ -477,15 +470,13 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
     W diag;
     if constexpr(kB) {
 #pragma unroll
-        for(int r = 0; r < R; ++r) H[r] = Narrow::state(-(i0 + lane * R + r + 1) * g, g);
-        diag = Narrow::state(-(i0 + lane * R) * g, g);
+        for(int r = 0; r < R; ++r) H[r] = 0u;   // column 0 of T
+        diag = 0u;
     } else {
 #pragma unroll
         for(int r = 0; r < R; ++r) H[r] = K::splat(-(i0 + lane * R + r + 1) * g);
         diag = K::splat(-(i0 + lane * R) * g);
     }
-    const W g2 = ((uint32_t) g & 0xffffu) * 0x10001u;
-    const W ng16 = ((uint32_t) (-g) & 0xffffu) * 0x10001u;
     W hlast = H[R - 1];
     uint32_t bq_cur = bound[lane], bq_nxt = bound[32 + lane];
     const uint32_t *prow = sprof + lane * 4;
@@ -509,8 +500,7 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
                 uint4 pw = *reinterpret_cast<const uint4 *>(pb);
                 W sc[4] = {(W) pw.x, (W) pw.y, (W) pw.z, (W) pw.w};
                 if constexpr(kB) {
-                    // Alternate rows: two maxes (one dependent op on the row
-                    // chain) and the three-way max (one ALU op); see Narrow.
+                    // T = max(T_left, T_up, T_diag + s + 2g); see Narrow.
                     W above = up, dprev = diag;
 #pragma unroll
                     for(int r = 0; r < R; ++r) {
@@ -520,8 +510,7 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
                         }
                         const W D = __vadd2(dprev, sc[r & 3]);
                         dprev = H[r];
-                        if(r % 2 == 0) H[r] = __viaddmax_u16x2(above, ng16, __viaddmax_u16x2(H[r], ng16, D));
-                        else H[r] = __vimax3_u16x2(H[r], above, D) - g2;
+                        H[r] = __vimax3_u16x2(H[r], above, D);
                         above = H[r];
                     }
                 } else {
@@ -595,11 +584,11 @@ __device__ __noinline__ void narrow_task(uint32_t *sprof, const int8_t *g1, uint
             __syncwarp();
             if(s == s2) {
                 const int rr = e2 - 1 - i0;
-                r2 = __shfl_sync(kFull, Narrow::hi(pick_row<R, Narrow>(H, rr % R), g), rr / R);
+                r2 = __shfl_sync(kFull, Narrow::hi(pick_row<R, Narrow>(H, rr % R), g, e2, ncols), rr / R);
             }
             if(last) {
                 const int rr = e1 - 1 - i0;
-                r1 = __shfl_sync(kFull, Narrow::lo(pick_row<R, Narrow>(H, rr % R), g), rr / R);
+                r1 = __shfl_sync(kFull, Narrow::lo(pick_row<R, Narrow>(H, rr % R), g, e1, ncols), rr / R);
             }
         }
     }
@@ -663,8 +652,8 @@ __device__ __forceinline__ void rows_pair_task(const JobView &jv, uint32_t k, ui
     const uint8_t *cols = jv.units + jv.uoff[y];
 
     if(jv.row_narrow[k]) {
-        // Row zero of the DP as the boundary above the first strip.
-        if(has) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = dev::Narrow::state(-(jj + 1) * jv.g, jv.g);
+        // Row zero of the DP (0 in the T state) as the boundary above the first strip.
+        if(has) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = 0u;
         int nst, R;
         dev::strip_plan<RMAX>(e1, nst, R);
         int32_t r1 = 0, r2 = 0;
@@ -829,18 +818,19 @@ static int occupancy(KernelT kernel, size_t smem, int *blocks)
     return 0;
 }
 
-// 16-bit lanes are exact when every value a task can produce fits them:
-// H(i,j) lies in [-g(i+j), max(smax,0)*min(i,j)] for all i <= rows (padded
-// strip rows included, whose scores are 0) and j <= cols, and the partial sums
-// (diag + s, left - g) reach at most max(g, |smin|) below the floor. The lane
-// state S = H - g + 0x8000 and the two-max form's S_diag + s must stay in
-// [0, 0xffff] with S >= g, which costs one more g of headroom below:
-// g(rows + cols) + g + max(g, |smin|) <= 32768.
+// 16-bit lanes are exact when every scored cell of a task fits them. In the
+// lane state T(i,j) = H(i,j) + g(i+j) every path scores the sum of s + 2g over
+// its matched cells, so with smin + 2g >= 0 the state and its diagonal
+// candidate lie in [0, min(i,j)*(smax + 2g)], with min(i,j) <= min(rows, cols).
+// Cells outside the sequences (padding rows, the shorter sequence's tail) may
+// wrap within their half but never feed a scored cell. Clean sequences hold
+// letter units only, so smin and smax are taken over the letter block.
 static inline bool narrow_ok(int64_t rows_p, int64_t cols, const ExtTable &t)
 {
-    const int64_t lo = (int64_t) t.penalty * (rows_p + cols + 1) + std::max<int64_t>(t.penalty, t.max_neg);
-    const int64_t hi = (int64_t) std::max<int32_t>(t.max_pos, 0) * std::min(rows_p, cols);
-    return lo <= 32768 && hi <= 32767;
+    const int64_t g2 = 2 * (int64_t) t.penalty;
+    if((int64_t) t.letter_neg > g2) return false;
+    const int64_t step = std::max<int64_t>((int64_t) t.letter_pos + g2, 0);
+    return step * std::min(rows_p, cols) <= 0xffff;
 }
 
 // Batched-kernel tile shapes: rows per lane R and warps per CTA W.

@@ -42,6 +42,10 @@ __device__ __forceinline__ uint32_t op(uint32_t a, uint32_t b, uint32_t c)
         const uint32_t ds = a + c;
         const uint32_t t = __viaddmax_u16x2(b, 0xfffdfffdu, ds);
         return __viaddmax_u16x2(a, 0xfffdfffdu, t);
+    } else if constexpr(OP == 14) {
+        // The 16x2 NW cell on the gap-free state T = H + g(i+j):
+        // max(T_left, T_up, T_diag + s + 2g).
+        return __vimax3_u16x2(a, b, __vadd2(b, c));
     } else {
         return a ^ b;
     }
@@ -71,6 +75,66 @@ __global__ void __launch_bounds__(256) probe_kernel(const uint32_t *__restrict__
     for(int k = 0; k < 8; ++k) acc ^= x[k];
     out[t] = acc;
     if(threadIdx.x == 0) atomicMax(cycles, c1 - c0);
+}
+
+// Shared-memory load bandwidth: every warp reads 512 contiguous bytes per
+// ld.shared.v4 (bank-conflict free, the access shape of the NW profile loads),
+// eight loads per iteration at addresses that change every iteration.
+// ops_per_clk_sm reports bytes per SM per clock.
+__global__ void __launch_bounds__(256) probe_lds_kernel(uint32_t *__restrict__ out, int iters,
+                                                        unsigned long long *cycles)
+{
+    __shared__ __align__(16) uint32_t buf[4096];   // 16 KB
+    for(int k = threadIdx.x; k < 4096; k += blockDim.x) buf[k] = k * 2654435761u;
+    __syncthreads();
+    const uint32_t base = (uint32_t) __cvta_generic_to_shared(buf) + (threadIdx.x & 31) * 16;
+    uint32_t acc = 0;
+    const unsigned long long c0 = clock64();
+    for(int it = 0; it < iters; ++it) {
+#pragma unroll
+        for(int k = 0; k < 8; ++k) {
+            const uint32_t addr = base + (uint32_t) (((it * 8 + k) & 31) * 512);
+            uint32_t x, y, z, w;
+            asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];" : "=r"(x), "=r"(y), "=r"(z), "=r"(w) : "r"(addr));
+            acc ^= x ^ y ^ z ^ w;
+        }
+    }
+    __syncthreads();
+    const unsigned long long c1 = clock64();
+    out[blockIdx.x * blockDim.x + threadIdx.x] = acc;
+    if(threadIdx.x == 0) atomicMax(cycles, c1 - c0);
+}
+
+static int run_lds(msa_ctx *ctx, int iters, msa_op_probe *res)
+{
+    const int threads = 256;
+    int per_sm = 0;
+    MSA_CUDA_TRY(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, probe_lds_kernel, threads, 0));
+    per_sm = std::min(per_sm, 4);
+    const int blocks = ctx->num_sms * per_sm;
+    MSA_CUDA_TRY(ctx, ctx->tasks.ensure((size_t) blocks * threads * 4 + 64));
+    uint32_t *out = (uint32_t *) ctx->tasks.ptr;
+    auto *cyc = (unsigned long long *) (out + (size_t) blocks * threads);
+    cudaStream_t s = ctx->stream;
+    for(int rep = 0; rep < 2; ++rep) {   // first pass warms up
+        MSA_CUDA_TRY(ctx, cudaMemsetAsync(cyc, 0, 8, s));
+        MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[0], s));
+        probe_lds_kernel<<<blocks, threads, 0, s>>>(out, iters, cyc);
+        MSA_CUDA_TRY(ctx, cudaGetLastError());
+        MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[1], s));
+        ctx->launches++;
+    }
+    unsigned long long cycles = 0;
+    MSA_CUDA_TRY(ctx, cudaMemcpyAsync(&cycles, cyc, 8, cudaMemcpyDeviceToHost, s));
+    MSA_CUDA_TRY(ctx, cudaStreamSynchronize(s));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, ctx->ev[0], ctx->ev[1]);
+    const double bytes_per_sm = (double) per_sm * threads * iters * 8.0 * 16.0;
+    res->ops_per_clk_sm = cycles ? bytes_per_sm / (double) cycles : 0.0;
+    res->ms = ms;
+    res->lane_ops = (uint64_t) ((double) blocks * threads * iters * 8.0);
+    res->sm_clock_mhz = ms > 0 ? (double) cycles / (ms * 1e3) : 0.0;
+    return MSA_OK;
 }
 
 template <int OP>
@@ -131,6 +195,8 @@ extern "C" int msa_probe_op(msa_ctx *ctx, int op, int iters, msa_op_probe *out)
         case 11: return run<11>(ctx, iters, out);
         case 12: return run<12>(ctx, iters, out);
         case 13: return run<13>(ctx, iters, out);
+        case 14: return run<14>(ctx, iters, out);
+        case 15: return run_lds(ctx, iters, out);
         default: return MSA_ERR_INVALID;
     }
 }

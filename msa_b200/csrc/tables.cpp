@@ -31,7 +31,7 @@ int make_ext_table(const msa_table *t, ExtTable *out, std::string *err)
 {
     std::memset(out, 0, sizeof(*out));
     out->penalty = t->penalty;
-    int32_t mx = 0, mpos = -128, mneg = 0;
+    int32_t mx = 0, mpos = -128, mneg = 0, lpos = -128, lneg = 0;
     for(int x = 0; x < kAlpha; ++x) {
         for(int y = 0; y < kAlpha; ++y) {
             int32_t v = 0;
@@ -56,6 +56,10 @@ int make_ext_table(const msa_table *t, ExtTable *out, std::string *err)
                 mpos = std::max(mpos, v);
                 if(v < 0) mneg = std::max(mneg, -v);
             }
+            if(ok && x < MSA_UNIT_END && y < MSA_UNIT_END) {
+                lpos = std::max(lpos, v);
+                if(v < 0) lneg = std::max(lneg, -v);
+            }
         }
     }
     if(t->penalty < 0 || t->penalty > (1 << 20)) {
@@ -65,6 +69,8 @@ int make_ext_table(const msa_table *t, ExtTable *out, std::string *err)
     out->max_abs = mx;
     out->max_pos = mpos;
     out->max_neg = mneg;
+    out->letter_pos = lpos;
+    out->letter_neg = lneg;
     return MSA_OK;
 }
 

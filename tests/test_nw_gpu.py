@@ -62,6 +62,18 @@ def test_random_sets_match_oracle(gpu, tables, mode, seed, n, lo, hi, table):
     assert np.array_equal(got, oracle_scores(wl, table, tables))
 
 
+@pytest.mark.parametrize("table", ["default", "blosum62", "blosum45", "blosum50", "blosum80", "blosum90", "pam250"])
+def test_named_tables_take_16bit_lanes(gpu, tables, table):
+    # Short sequences of letters fit the 16-bit lanes under every named table
+    # (each table's letter block has smin = -g); the batched kernel must run
+    # them there and stay exact.
+    alpha = b"ACGTN" if table == "default" else b"ARNDCQEGHILKMFPSTWYVBZX"
+    wl = W.random_set(60, 24, 200, 900, alphabet=alpha)
+    got = gpu_scores(wl, table, _lib.MSA_NW_PERSISTENT)
+    assert pairwise.last_stats().narrow_tasks > 0
+    assert np.array_equal(got, oracle_scores(wl, table, tables))
+
+
 def test_plain_and_persistent_agree_on_related_sequences(gpu):
     wl = W.c2(n=300)
     a = gpu_scores(wl, "blosum62", _lib.MSA_NW_PLAIN)
@@ -249,21 +261,27 @@ def test_parts_on_device_into_one_buffer(gpu):
 
 @pytest.mark.parametrize("mode", MODES)
 def test_16bit_lanes_near_their_bound(gpu, golden, mode):
-    # Gaps cost 1 and mismatches 60, so an all-A against an all-C sequence is
-    # scored by the all-gap path: H at the far corner is -(L1 + L2), within a
-    # few hundred of the 16-bit lanes' floor; the batched kernel must still
-    # take them (narrow_tasks) and stay exact. A longer pair must fall back to
-    # 32-bit lanes.
+    # The 16-bit lanes hold T = H + g(i+j), the sum of s + 2g over an
+    # alignment's matched cells. Matches +1, mismatches -2 and gap 1 make
+    # s + 2g either 3 or 0: all-A against all-A drives T to 3*lc (0xffff at
+    # lc = 21845, the largest column count the bound admits) and all-A against
+    # all-C keeps it at 0, the floor. One more column must fall back to 32-bit
+    # lanes, and so must a table whose mismatch costs more than two gaps.
+    m = np.full((25, 25), -2, np.int32)
+    np.fill_diagonal(m, 1)
+    edge = ScoringTable.custom(m, 1)
     m = np.full((25, 25), -60, np.int32)
     np.fill_diagonal(m, 1)
-    table = ScoringTable.custom(m, 1)
-    for la, lc, narrow in ((16380, 15999, True), (16383, 16383, False)):
-        seqs = [b"A" * la, b"C" * lc, b"A" * (lc - 3)]
+    steep = ScoringTable.custom(m, 1)
+    for table, lc, narrow in ((edge, 21845, True), (edge, 21846, False), (steep, 4000, False)):
+        la = lc + 7
+        seqs = [b"A" * la, b"A" * lc, b"C" * (lc - 3)]
         wl = W.Workload("edge", [np.frombuffer(s, np.uint8) for s in seqs], "default", 0)
         flat, offs, lens = wl.flat_units()
         got = pairwise.score_units(flat, offs, lens, table, mode)
-        # (1,0): all gaps; (2,0): lc-3 matches then la-(lc-3) gaps; (2,1): all gaps
-        want = np.array([-(la + lc), (lc - 3) - (la - (lc - 3)), -(lc + lc - 3)], np.int32)
-        assert np.array_equal(got, want), (la, lc, got, want)
+        # (1,0): lc matches and 7 gaps; (2,0) and (2,1): every letter against a
+        # gap or a mismatch (a mismatch costs at least two gaps).
+        want = np.array([lc - (la - lc), -(la + lc - 3), -(lc + lc - 3)], np.int32)
+        assert np.array_equal(got, want), (lc, got, want)
         if mode == _lib.MSA_NW_PERSISTENT:
-            assert (pairwise.last_stats().narrow_tasks > 0) == narrow
+            assert (pairwise.last_stats().narrow_tasks > 0) == narrow, lc
