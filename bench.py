@@ -328,8 +328,16 @@ def serve_bench(args):
         for w in [float(x) for x in args.sweep_windows.split(",")]:
             for seed in seeds:
                 lat, agg, st = run_server(w, arrival_times(seed))
+                slow = np.argsort(lat)[::-1][:4]
+                t0 = min(x["submit_ms"] for x in st)
+                tail = [{"latency_ms": round(float(lat[k]), 1), "submit_ms": round(st[k]["submit_ms"] - t0, 1),
+                         "admit_wait_ms": round(st[k]["admit_ms"] - st[k]["submit_ms"], 1),
+                         "run_ms": round(st[k]["done_ms"] - st[k]["admit_ms"], 1), "cells": int(st[k]["cells"])}
+                        for k in slow]
                 print(json.dumps({"window_ms": w, "arrival_seed": seed, **summary(lat, agg, st),
-                                  "saturated_gcups": sat_gcups, "arrival_rate_per_s": rate}), flush=True)
+                                  "p90_ms": float(np.percentile(lat, 90)), "max_ms": float(lat.max()),
+                                  "saturated_gcups": sat_gcups, "arrival_rate_per_s": rate, "slowest": tail}),
+                      flush=True)
         return None
 
     continuous = summary(*run_server())

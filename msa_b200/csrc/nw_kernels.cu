@@ -416,7 +416,9 @@ namespace dev {
 
 // Stages strip rows [i0, i0 + 32R) as 32-bit profile words in shared memory,
 // laid out [code][plane of 4 rows][lane][4 words] so that one 16-byte load per
-// lane and plane is bank-conflict free for any codes the lanes hold.
+// lane and plane is bank-conflict free for any codes the lanes hold. When R is
+// 2 mod 4 (16-bit lanes only), each lane's last two rows form a half plane
+// [code][lane][2 words] after the full ones, read with one 8-byte load.
 // Narrow: word = (s(X1_i, b) + 2g, s(X2_i, b) + 2g) as 16x2 (see Narrow);
 // rows of X2 past its profile (lp2) score 0. Wide: word = s(X1_i, b) as int32.
 template <int R, bool kNarrow>
@@ -425,6 +427,25 @@ __device__ __forceinline__ void stage_words(uint32_t *sprof, const int8_t *__res
 {
     const uint32_t gg = ((uint32_t) (2 * gap) & 0xffffu) * 0x10001u;
     constexpr int SH = 32 * R;
+    if constexpr(R % 4 != 0) {
+        static_assert(kNarrow && R % 2 == 0, "half planes are staged for 16-bit lanes only");
+        constexpr int G2 = SH / 2;       // 2-row groups per code row
+        constexpr int P = R / 4;         // full planes per lane
+        for(int c = threadIdx.x; c < kAlpha * G2; c += blockDim.x) {
+            const int b = c / G2, q = c - b * G2;
+            const uint32_t va = __ldg(reinterpret_cast<const uint16_t *>(g1 + (size_t) b * lp1 + i0) + q);
+            uint32_t vb = 0;
+            if((uint32_t) (i0 + 2 * q) < lp2) vb = __ldg(reinterpret_cast<const uint16_t *>(g2 + (size_t) b * lp2 + i0) + q);
+            const int row = 2 * q, ln = row / R, r = row - ln * R;
+            uint2 o;
+            o.x = __vadd2(sbyte2<0>(va, vb), gg);
+            o.y = __vadd2(sbyte2<1>(va, vb), gg);
+            uint32_t *dst = r < 4 * P ? sprof + b * SH + (r >> 2) * 128 + ln * 4 + (r & 3)
+                                      : sprof + b * SH + P * 128 + ln * 2;
+            *reinterpret_cast<uint2 *>(dst) = o;
+        }
+        return;
+    } else {
     constexpr int G = SH / 4;        // 4-row groups per code row
     constexpr int PL = R / 4;        // planes per lane
     for(int c = threadIdx.x; c < kAlpha * G; c += blockDim.x) {
@@ -446,6 +467,7 @@ __device__ __forceinline__ void stage_words(uint32_t *sprof, const int8_t *__res
             o.w = (uint32_t) sbyte<3>(va);
         }
         *reinterpret_cast<uint4 *>(sprof + b * SH + pl * 128 + ln * 4) = o;
+    }
     }
 }
 
@@ -480,6 +502,8 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
     W hlast = H[R - 1];
     uint32_t bq_cur = bound[lane], bq_nxt = bound[32 + lane];
     const uint32_t *prow = sprof + lane * 4;
+    constexpr int P = R / 4;                      // full profile planes per lane
+    const int half_off = P * 128 - lane * 2;      // half plane (R % 4 == 2) from prow
     const bool st31 = store_bound && lane == 31;
     int j = -lane;
     uint32_t cur = cols[j], nxt = cols[j + 1];   // columns -32..ncols+35 lie in the padded store
@@ -497,23 +521,30 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
             if(lane == 0) up = (W) bv;
             if(!kG || (unsigned) j < (unsigned) ncols) {
                 const uint32_t *pb = prow + cur * SH;
-                uint4 pw = *reinterpret_cast<const uint4 *>(pb);
-                W sc[4] = {(W) pw.x, (W) pw.y, (W) pw.z, (W) pw.w};
+                W sc[4];
+                auto load_plane = [&](int q) {
+                    if(q < P) {
+                        const uint4 v = *reinterpret_cast<const uint4 *>(pb + q * 128);
+                        sc[0] = (W) v.x; sc[1] = (W) v.y; sc[2] = (W) v.z; sc[3] = (W) v.w;
+                    } else {
+                        const uint2 v = *reinterpret_cast<const uint2 *>(pb + half_off);
+                        sc[0] = (W) v.x; sc[1] = (W) v.y;
+                    }
+                };
+                load_plane(0);
                 if constexpr(kB) {
                     // T = max(T_left, T_up, T_diag + s + 2g); see Narrow.
                     W above = up, dprev = diag;
 #pragma unroll
                     for(int r = 0; r < R; ++r) {
-                        if(r > 0 && (r & 3) == 0) {
-                            pw = *reinterpret_cast<const uint4 *>(pb + (r >> 2) * 128);
-                            sc[0] = (W) pw.x; sc[1] = (W) pw.y; sc[2] = (W) pw.z; sc[3] = (W) pw.w;
-                        }
+                        if(r > 0 && (r & 3) == 0) load_plane(r >> 2);
                         const W D = __vadd2(dprev, sc[r & 3]);
                         dprev = H[r];
                         H[r] = __vimax3_u16x2(H[r], above, D);
                         above = H[r];
                     }
                 } else {
+                static_assert(R % 4 == 0, "32-bit lanes use full planes");
                 // Row r needs the old H[r-1] (diagonal) and old H[r] (left): the
                 // off-chain part for row r+1 is computed before row r is
                 // overwritten, so no register copies are needed.
@@ -523,10 +554,7 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
                 for(int r = 0; r < R; ++r) {
                     const W pr = pn;
                     if(r + 1 < R) {
-                        if(((r + 1) & 3) == 0) {
-                            pw = *reinterpret_cast<const uint4 *>(pb + ((r + 1) >> 2) * 128);
-                            sc[0] = (W) pw.x; sc[1] = (W) pw.y; sc[2] = (W) pw.z; sc[3] = (W) pw.w;
-                        }
+                        if(((r + 1) & 3) == 0) load_plane((r + 1) >> 2);
                         pn = K::cell_part(H[r], sc[(r + 1) & 3], H[r + 1], ng);
                     }
                     H[r] = K::cell_chain(u_, ng, pr);
@@ -622,13 +650,13 @@ __device__ __noinline__ void wide_task(uint32_t *sprof, const int8_t *g1, uint32
 }
 
 // Strip plan for `rows` rows with at most 32*RMAX rows per strip: the fewest
-// strips, each of 32R rows with R the smallest multiple of 4 that covers them.
+// strips, each of 32R rows with R the smallest even number that covers them.
 template <int RMAX>
 __device__ __forceinline__ void strip_plan(int rows, int &nst, int &R)
 {
     nst = (rows + 32 * RMAX - 1) / (32 * RMAX);
     R = (rows + 32 * nst - 1) / (32 * nst);
-    R = (R + 3) & ~3;
+    R = (R + 1) & ~1;
 }
 
 }  // namespace dev
@@ -661,10 +689,14 @@ __device__ __forceinline__ void rows_pair_task(const JobView &jv, uint32_t k, ui
         const uint32_t lp1 = jv.plp[x1], lp2 = jv.plp[x2];
 #define MSA_NARROW(RR) case RR: dev::narrow_task<RR>(sprof_b, g1, lp1, g2, lp2, e1, e2, nst, has, cols, ncols, bound, jv.g, lane, r1, r2); break;
         switch(R) {
-            MSA_NARROW(4) MSA_NARROW(8) MSA_NARROW(12) MSA_NARROW(16)
+            MSA_NARROW(2) MSA_NARROW(4) MSA_NARROW(6) MSA_NARROW(8) MSA_NARROW(10) MSA_NARROW(12) MSA_NARROW(14)
+            MSA_NARROW(16)
             default:
                 if constexpr(RMAX > 16) {
-                    switch(R) { MSA_NARROW(20) MSA_NARROW(24) MSA_NARROW(28) MSA_NARROW(32) default: break; }
+                    switch(R) {
+                        MSA_NARROW(18) MSA_NARROW(20) MSA_NARROW(22) MSA_NARROW(24) MSA_NARROW(26) MSA_NARROW(28)
+                        MSA_NARROW(30) MSA_NARROW(32) default: break;
+                    }
                 }
                 break;
         }
