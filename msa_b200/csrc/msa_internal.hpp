@@ -170,6 +170,7 @@ struct ServeLaunch {
     unsigned long long *counter;
 };
 int serve_grid(msa_ctx *ctx, uint64_t *grid);
+cudaError_t load_profiles_kernel();   // loads the profile kernel's code on the current device
 cudaError_t launch_serve(const ServeLaunch &l, uint64_t grid, cudaStream_t s);
 size_t job_view_bytes();
 void fill_job_view(void *dst, const SeqStore *st, const int8_t *d_prof, const uint8_t *d_narrow, int32_t *d_out,

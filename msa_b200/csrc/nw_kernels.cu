@@ -916,6 +916,12 @@ void fill_job_view(void *dst, const SeqStore *st, const int8_t *d_prof, const ui
     std::memcpy(dst, &v, sizeof(v));
 }
 
+cudaError_t load_profiles_kernel()
+{
+    cudaFuncAttributes a{};
+    return cudaFuncGetAttributes(&a, build_profiles_kernel);
+}
+
 int serve_grid(msa_ctx *ctx, uint64_t *grid)
 {
     auto kern = nw_serve_kernel<32, 8>;

@@ -96,13 +96,14 @@ struct msa_server {
     std::vector<msa::Job *> admitted;
     std::map<uint64_t, msa::Job *> jobs;
     bool stop = false;
+    bool worker_ready = false;   // the launch thread has its staging buffers
     uint64_t next_id = 1;
     uint64_t budget = 0, used = 0;
     uint32_t max_jobs = 64, quantum = 0;
     double window_ms = 0;   // admission window (0 = admit at once)
     double t0 = 0;
     // launch resources (worker thread only)
-    msa::DevBuf bound, tasks, views, counter, tasks2, views2, counter2;
+    msa::DevBuf bound, tasks, views, counter, bound2, tasks2, views2, counter2;
     uint64_t bound_stride = 0, grid = 0;
     std::vector<uint32_t> h_tasks;
     std::vector<uint8_t> h_views;
@@ -347,13 +348,29 @@ void worker_loop(msa_server *srv)
 {
     msa_ctx *ctx = srv->ctx;
     cudaSetDevice(ctx->device);
-    cudaStream_t compute = ctx->own_stream, drain = nullptr;
+    // The two launches in flight run on two streams with their own boundary
+    // rows, so the next launch's CTAs fill the SMs that the previous launch's
+    // last tasks leave idle. Their tasks are disjoint pairs.
+    cudaStream_t compute2 = nullptr, drain = nullptr;
+    cudaStreamCreateWithFlags(&compute2, cudaStreamNonBlocking);
     cudaStreamCreateWithFlags(&drain, cudaStreamNonBlocking);
-    // Job memory goes back to the pool on the admission stream, where the next
-    // admissions reuse it without waiting for this thread's launches.
-    cudaStream_t release_stream = srv->adm->stream;
+    const cudaStream_t slot_stream[2] = {ctx->own_stream, compute2};
+    // Job memory goes back to the pool on this thread's own copy stream, never
+    // on the admission stream: the admission thread may be capturing a CUDA
+    // graph there (jobs scored in the reference's orientation), and a free
+    // enqueued on a capturing stream would become part of that graph. The pool
+    // hands the memory to the next admissions once the free has completed.
+    const cudaStream_t release_stream = drain;
     InFlight slots[2];
-    for(auto &f : slots) cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming);
+    for(auto &f : slots) {
+        cudaEventCreateWithFlags(&f.done, cudaEventDisableTiming);
+        f.stage(1 << 20, 64 << 10);   // pinned staging before the first job
+    }
+    {
+        std::lock_guard<std::mutex> lk(srv->mu);
+        srv->worker_ready = true;
+    }
+    srv->cv_done.notify_all();
     int cur = 0;
     const size_t vb = job_view_bytes();
 
@@ -450,8 +467,9 @@ void worker_loop(msa_server *srv)
         const uint64_t stride = round_up(max_cols + 160, 32);
         if(!srv->grid && serve_grid(ctx, &srv->grid)) break;
         if(stride > srv->bound_stride) {
-            retire(slots[cur ^ 1]);   // the buffer is about to move
-            if(srv->bound.ensure(srv->grid * kServeTiles.W * std::max<uint64_t>(stride, 2048 + 160) * 4)) break;
+            retire(slots[cur ^ 1]);   // the buffers are about to move
+            const uint64_t bytes = srv->grid * kServeTiles.W * std::max<uint64_t>(stride, 2048 + 160) * 4;
+            if(srv->bound.ensure(bytes) || srv->bound2.ensure(bytes)) break;
             srv->bound_stride = std::max<uint64_t>(stride, 2048 + 160);
         }
         struct T { uint32_t slot, k, g; uint64_t cost; };
@@ -488,7 +506,8 @@ void worker_loop(msa_server *srv)
         std::memcpy(f.h_views, srv->h_views.data(), srv->h_views.size());
         // Device buffers of this slot: grow only while nothing else is in flight.
         DevBuf &tb = cur ? srv->tasks : srv->tasks2, &vbuf = cur ? srv->views : srv->views2,
-               &cb = cur ? srv->counter : srv->counter2;
+               &cb = cur ? srv->counter : srv->counter2, &bb = cur ? srv->bound2 : srv->bound;
+        const cudaStream_t compute = slot_stream[cur];
         if(tb.bytes < ntasks * 16 + 16 || vbuf.bytes < srv->h_views.size() + 16) retire(slots[cur ^ 1]);
         cudaError_t e = tb.ensure(std::max<size_t>(ntasks * 16 + 16, 1 << 20));
         if(!e) e = vbuf.ensure(std::max<size_t>(srv->h_views.size() + 16, 64 << 10));
@@ -497,7 +516,7 @@ void worker_loop(msa_server *srv)
         if(!e) e = cudaMemcpyAsync(vbuf.ptr, f.h_views, srv->h_views.size(), cudaMemcpyHostToDevice, compute);
         if(!e) e = cudaMemsetAsync(cb.ptr, 0, 64, compute);
         if(!e) {
-            ServeLaunch L{vbuf.ptr, tb.ptr, ntasks, (uint32_t *) srv->bound.ptr, srv->bound_stride,
+            ServeLaunch L{vbuf.ptr, tb.ptr, ntasks, (uint32_t *) bb.ptr, srv->bound_stride,
                           (unsigned long long *) cb.ptr};
             e = launch_serve(L, srv->grid, compute);
             ctx->launches++;
@@ -511,6 +530,47 @@ void worker_loop(msa_server *srv)
     retire(slots[1]);
     for(auto &f : slots) { cudaEventDestroy(f.done); f.release(); }
     cudaStreamDestroy(drain);
+    cudaStreamDestroy(compute2);
+}
+
+// Pays a server's one-time costs before it takes jobs, so that they do not
+// fall on the first jobs' latency: the job-memory pool grows to hold up to
+// 2 GiB (released memory stays in the pool), both launch slots get their
+// boundary rows (sequences up to 2,048 units; longer ones grow them later)
+// and task tables, and the serving kernel runs once on an empty task list.
+int warm_server(msa_server *srv)
+{
+    msa_ctx *ctx = srv->ctx;
+    cudaSetDevice(ctx->device);
+    const uint64_t warm = std::min<uint64_t>(srv->budget, 2ull << 30);
+    if(srv->pool && warm) {
+        void *p = nullptr;
+        cudaError_t e = cudaMallocFromPoolAsync(&p, warm, srv->pool, srv->adm->stream);
+        if(!e) e = cudaFreeAsync(p, srv->adm->stream);
+        if(!e) e = cudaStreamSynchronize(srv->adm->stream);
+        if(e) return cuda_error(srv->adm, e, "job memory pool");
+    }
+    if(const int rc = serve_grid(ctx, &srv->grid)) return rc;
+    const uint64_t stride = 2048 + 160;
+    const uint64_t bytes = srv->grid * kServeTiles.W * stride * 4;
+    cudaError_t e = srv->bound.ensure(bytes);
+    if(!e) e = srv->bound2.ensure(bytes);
+    if(!e) e = srv->tasks.ensure(1 << 20);
+    if(!e) e = srv->tasks2.ensure(1 << 20);
+    if(!e) e = srv->views.ensure(64 << 10);
+    if(!e) e = srv->views2.ensure(64 << 10);
+    if(!e) e = srv->counter.ensure(64);
+    if(!e) e = srv->counter2.ensure(64);
+    if(e) return cuda_error(ctx, e, "serving buffers");
+    srv->bound_stride = stride;
+    e = cudaMemsetAsync(srv->counter.ptr, 0, 64, ctx->own_stream);
+    const ServeLaunch L{srv->views.ptr, srv->tasks.ptr, 0, (uint32_t *) srv->bound.ptr, stride,
+                        (unsigned long long *) srv->counter.ptr};
+    if(!e) e = launch_serve(L, srv->grid, ctx->own_stream);
+    if(!e) e = load_profiles_kernel();
+    if(!e) e = cudaStreamSynchronize(ctx->own_stream);
+    if(e) return cuda_error(ctx, e, "serving warm-up");
+    return MSA_OK;
 }
 
 }  // namespace
@@ -567,8 +627,29 @@ int msa_serve_start(const msa_serve_config *cfg, msa_server **out)
         srv->max_jobs = cfg->max_jobs ? cfg->max_jobs : 64;
         srv->quantum = cfg->quantum_mcells;
         srv->window_ms = cfg->batch_window_us / 1000.0;
-        srv->t0 = now_ms();
+        rc = warm_server(srv);
+        if(rc) {
+            srv->bound.release();
+            srv->bound2.release();
+            srv->tasks.release();
+            srv->tasks2.release();
+            srv->views.release();
+            srv->views2.release();
+            srv->counter.release();
+            srv->counter2.release();
+            msa_destroy(srv->adm);
+            if(srv->adm_stream) cudaStreamDestroy(srv->adm_stream);
+            msa_destroy(srv->ctx);
+            if(srv->pool) cudaMemPoolDestroy(srv->pool);
+            delete srv;
+            return rc;
+        }
         srv->worker = std::thread(worker_loop, srv);
+        {
+            std::unique_lock<std::mutex> lk(srv->mu);
+            srv->cv_done.wait(lk, [srv] { return srv->worker_ready; });
+        }
+        srv->t0 = now_ms();
         srv->admitter = std::thread(admission_loop, srv);
         *out = srv;
         return MSA_OK;
@@ -681,6 +762,7 @@ int msa_serve_stop(msa_server *srv)
     }
     cudaStreamSynchronize(srv->adm->stream);
     srv->bound.release();
+    srv->bound2.release();
     srv->tasks.release();
     srv->views.release();
     srv->counter.release();

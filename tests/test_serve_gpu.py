@@ -115,3 +115,25 @@ def test_windowed_admission_starts_jobs_on_window_boundaries(gpu):
         assert np.array_equal(scores, _alone(wl))
         boundary = np.ceil(stats["submit_ms"] / window) * window
         assert stats["admit_ms"] >= boundary - 1e-3
+
+
+def test_reference_orientation_jobs_interleaved_with_resident_jobs(gpu):
+    """Jobs with END units are scored at admission, in the reference's
+    orientation, on the admission stream (which may capture a CUDA graph for
+    them) while merged launches finish other jobs. Finished jobs' memory must
+    not be released on that stream: a release enqueued during a capture would
+    become part of the graph and the job's scores or memory would be lost.
+    Several rounds of such jobs interleaved with resident ones, every job equal
+    to the job alone."""
+    for rnd in range(3):
+        jobs = []
+        for k in range(6):
+            wl = W.c5_job(6000 + 10 * rnd + k)
+            wl.seqs = wl.seqs[:80]
+            jobs.append(wl)
+            jobs.append(W.random_set(600 + 10 * rnd + k, 24, 0, 260, extra=b"*\r"))
+        with Server(device=0) as srv:
+            ids = [srv.submit_workload(wl) for wl in jobs]
+            results = [srv.wait(i) for i in ids]
+        for wl, (scores, _) in zip(jobs, results):
+            assert np.array_equal(scores, _alone(wl)), (rnd, wl.name)
