@@ -235,6 +235,31 @@ PROBE_OPS = ["iadd", "imnmx", "viaddmax_s32", "vimax3_s32", "vadd2", "viaddmax_s
              "cell_u16x2_gapfree", "lds128_bytes"]
 
 
+def packed_row_fraction(wl, rmax: int = 32) -> float:
+    """Share of the DP cells that the batched kernel scores from packed-byte
+    profile rows, by replaying its plan: length-sorted sequences paired into
+    rows pairs, strips of 32R rows (R even, at most rmax), and 8 floor(R/16)
+    of each lane's R rows packed. Cells are weighted by the pair's unpadded
+    cells."""
+    e = np.sort(wl.lengths().astype(np.int64))[::-1]
+    n = len(e)
+    csum = np.concatenate([[0], np.cumsum(e)])       # csum[i] = sum of e[:i]
+    packed = total = 0.0
+    for k in range((n + 1) // 2):
+        a1, a2 = 2 * k, min(2 * k + 1, n - 1)
+        cols = float(csum[n] - csum[2 * k + 1])       # columns: sorted 2k+1 .. n-1
+        if cols <= 0:
+            continue
+        e1 = int(e[a1])
+        nst = -(-e1 // (32 * rmax))
+        r = -(-e1 // (32 * nst))
+        r = (r + 1) & ~1
+        cells = (e1 + (int(e[a2]) if a2 != a1 else 0)) * cols
+        packed += cells * (8 * (r // 16)) / r
+        total += cells
+    return packed / total if total else 0.0
+
+
 def probe_rate(ctx, op: int, iters: int = 2048) -> float:
     """Lane-ops (op 15: shared-memory bytes) per SM per clock of one probe form."""
     import ctypes
@@ -646,14 +671,20 @@ def main():
         props = torch.cuda.get_device_properties(local)
         sm_mhz = clocks.get("sm_mhz") or 1965.0
         nsm = props.multi_processor_count
-        # Ceilings of the batched kernel's cell, from rates measured here per SM
-        # clock (msa_probe_op): each 16x2 lane-op of the cell form updates two
-        # cells, and every cell reads one 16-bit profile half (2 bytes) from
-        # shared memory. The shared-memory one is the lowest: the roofline.
+        # Ceilings of the batched kernel from rates measured here per SM clock
+        # (msa_probe_op). A cell reads its score from shared memory: 2 bytes in
+        # a 16-bit profile row, 1 byte in a packed row (a share f of the cells,
+        # from the kernel's plan), so 2 - f bytes per cell. The ALU pipe
+        # (64 lanes/clk/SM) carries one vimax3 per two cells and one PRMT per
+        # two cells of a packed row: (1 + f) / 2 lane-ops per cell. The lower
+        # of the two is the roofline.
         lds = probe_rate(ctx, 15)
         cell_ops = probe_rate(ctx, 14)
-        smem_peak = nsm * (lds / 2.0) * sm_mhz * 1e6 / 1e9
+        f_packed = packed_row_fraction(wl)
+        smem_peak = nsm * (lds / (2.0 - f_packed)) * sm_mhz * 1e6 / 1e9
+        alu_peak = nsm * (64.0 / ((1.0 + f_packed) / 2.0)) * sm_mhz * 1e6 / 1e9
         cell_peak = nsm * (2.0 * cell_ops) * sm_mhz * 1e6 / 1e9
+        roof = min(smem_peak, alu_peak)
         # The four-op int32 issue figure (two max operations per cell on the ALU
         # pipe, 64 lanes/clk/SM): 32 cells/clk/SM.
         peak = nsm * 64 * sm_mhz * 1e6 / 2 / 1e9
@@ -680,16 +711,18 @@ def main():
                     "h2d_bytes_per_step": int(flat.nbytes + offs.nbytes + lens.nbytes),
                     "d2h_bytes_per_step": int(npairs * 4), "scores_match": e2e_ok},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "smem", "achieved": kernel_gcups, "peak": smem_peak, "unit": "GCUPS",
-                         "frac": kernel_gcups / smem_peak, "traffic": traffic,
+            "roofline": {"bound": "smem" if smem_peak <= alu_peak else "alu", "achieved": kernel_gcups,
+                         "peak": roof, "unit": "GCUPS", "frac": kernel_gcups / roof, "traffic": traffic,
                          "frac_int32_issue": kernel_gcups / peak,
-                         "ceilings_gcups": {"smem_profile_reads": smem_peak, "cell_ops_16x2": cell_peak,
-                                            "int32_issue_4ops_per_cell": peak},
+                         "packed_row_fraction": f_packed,
+                         "ceilings_gcups": {"smem_profile_reads": smem_peak, "alu_pipe": alu_peak,
+                                            "cell_ops_16x2_probe": cell_peak, "int32_issue_4ops_per_cell": peak},
                          "measured_per_sm_clk": {"lds_bytes": lds, "cell_16x2_lane_ops": cell_ops},
-                         "peak_basis": f"{nsm} SM x {lds:.1f} shared-memory bytes/clk (measured, ld.shared.v4) / "
-                                       f"2 bytes of profile per cell x {sm_mhz:.0f} MHz (median sampled); "
-                                       f"frac_int32_issue is against {nsm} SM x 64 ALU lanes/clk / 2 max-ops "
-                                       f"per cell"},
+                         "peak_basis": f"min of {nsm} SM x {lds:.1f} shared-memory bytes/clk (measured, "
+                                       f"ld.shared.v4) / (2 - {f_packed:.3f}) bytes of profile per cell and "
+                                       f"{nsm} SM x 64 ALU lanes/clk / ((1 + {f_packed:.3f}) / 2) lane-ops per cell, "
+                                       f"x {sm_mhz:.0f} MHz (median sampled); frac_int32_issue is against "
+                                       f"{nsm} SM x 64 ALU lanes/clk / 2 max-ops per cell"},
             "clocks": clocks,
             "cpu_baseline": cpu,
         }

@@ -414,23 +414,52 @@ struct ServeParams {
 
 namespace dev {
 
-// Stages strip rows [i0, i0 + 32R) as 32-bit profile words in shared memory,
-// laid out [code][plane of 4 rows][lane][4 words] so that one 16-byte load per
-// lane and plane is bank-conflict free for any codes the lanes hold. When R is
-// 2 mod 4 (16-bit lanes only), each lane's last two rows form a half plane
-// [code][lane][2 words] after the full ones, read with one 8-byte load.
-// Narrow: word = (s(X1_i, b) + 2g, s(X2_i, b) + 2g) as 16x2 (see Narrow);
-// rows of X2 past its profile (lp2) score 0. Wide: word = s(X1_i, b) as int32.
+// Shared-memory layout of one strip's profile for R rows per lane, per code:
+// R16 rows as 32-bit words in planes [lane][4 words] of 4 rows (one 16-byte
+// load per lane and plane, bank-conflict free whatever codes the lanes hold),
+// then a half plane [lane][2 words] when R16 is 2 mod 4; then, on 16-bit lanes,
+// R8 rows as packed bytes, one word holding rows r and r + 1 of both sequences,
+// in planes [lane][4 words] of 8 rows and a half plane [lane][2 words] of 4
+// rows when R8 is 4 mod 8. A packed row costs one PRMT (ALU pipe) and half the
+// shared-memory bytes of a 16-bit row. R8 = 8 floor(R/16) (a third to a half of
+// a long strip's rows) balances the shared-memory data pipe, the bound of
+// 16-bit rows alone, against the ALU pipe and issue: on c3 it measured 16.07
+// TCUPS against 14.81 with no packed rows and 15.96 with R8 = 4 floor(R/8).
+template <int R, bool kNarrow> struct Layout {
+    static constexpr int R8 = kNarrow ? 8 * (R / 16) : 0;
+    static constexpr int R16 = R - R8;
+    static constexpr int P16 = R16 / 4;                      // full 16-bit planes
+    static constexpr bool kHalf = R16 % 4 != 0;
+    static constexpr int HALF = P16 * 128;                   // word offset of the 16-bit half plane
+    static constexpr int PACK = HALF + (kHalf ? 64 : 0);     // word offset of the packed planes
+    static constexpr int P8 = R8 / 8;                        // full packed planes
+    static constexpr int PHALF = PACK + P8 * 128;            // word offset of the packed half plane
+    static constexpr int SH = PHALF + (R8 % 8 ? 64 : 0);     // words per code
+};
+
+// PRMT of w with a zero second operand.
+template <int SEL>
+__device__ __forceinline__ uint32_t prmt0(uint32_t w)
+{
+    uint32_t r;
+    asm("prmt.b32 %0, %1, 0, %2;" : "=r"(r) : "r"(w), "n"(SEL));
+    return r;
+}
+
+// Stages strip rows [i0, i0 + 32R) of the profile in shared memory (Layout).
+// Narrow: word = (s(X1_i, b) + 2g, s(X2_i, b) + 2g) as 16x2 (see Narrow), or
+// bytes (s1_i, s1_i+1, s2_i, s2_i+1) + 2g in the packed planes; rows of X2 past
+// its profile (lp2) score 0. Wide: word = s(X1_i, b) as int32.
 template <int R, bool kNarrow>
 __device__ __forceinline__ void stage_words(uint32_t *sprof, const int8_t *__restrict__ g1, uint32_t lp1,
                                             const int8_t *__restrict__ g2, uint32_t lp2, int i0, int32_t gap = 0)
 {
-    const uint32_t gg = ((uint32_t) (2 * gap) & 0xffffu) * 0x10001u;
-    constexpr int SH = 32 * R;
-    if constexpr(R % 4 != 0) {
-        static_assert(kNarrow && R % 2 == 0, "half planes are staged for 16-bit lanes only");
-        constexpr int G2 = SH / 2;       // 2-row groups per code row
-        constexpr int P = R / 4;         // full planes per lane
+    using L = Layout<R, kNarrow>;
+    constexpr int SH = L::SH;
+    if constexpr(kNarrow) {
+        static_assert(R % 2 == 0, "16-bit lanes take an even number of rows");
+        const uint32_t gg = ((uint32_t) (2 * gap) & 0xffffu) * 0x10001u;
+        constexpr int G2 = 16 * R;       // 2-row groups per code row (32R rows)
         for(int c = threadIdx.x; c < kAlpha * G2; c += blockDim.x) {
             const int b = c / G2, q = c - b * G2;
             const uint32_t va = __ldg(reinterpret_cast<const uint16_t *>(g1 + (size_t) b * lp1 + i0) + q);
@@ -440,34 +469,34 @@ __device__ __forceinline__ void stage_words(uint32_t *sprof, const int8_t *__res
             uint2 o;
             o.x = __vadd2(sbyte2<0>(va, vb), gg);
             o.y = __vadd2(sbyte2<1>(va, vb), gg);
-            uint32_t *dst = r < 4 * P ? sprof + b * SH + (r >> 2) * 128 + ln * 4 + (r & 3)
-                                      : sprof + b * SH + P * 128 + ln * 2;
-            *reinterpret_cast<uint2 *>(dst) = o;
+            uint32_t *code = sprof + b * SH;
+            if(r < 4 * L::P16) {
+                *reinterpret_cast<uint2 *>(code + (r >> 2) * 128 + ln * 4 + (r & 3)) = o;
+            } else if(r < L::R16) {
+                *reinterpret_cast<uint2 *>(code + L::HALF + ln * 2) = o;
+            } else {
+                const int wi = (r - L::R16) >> 1;   // packed word of rows r, r + 1
+                uint32_t pk;
+                asm("prmt.b32 %0, %1, %2, 0x6240;" : "=r"(pk) : "r"(o.x), "r"(o.y));
+                if(wi < 4 * L::P8) code[L::PACK + (wi >> 2) * 128 + ln * 4 + (wi & 3)] = pk;
+                else code[L::PHALF + ln * 2 + (wi - 4 * L::P8)] = pk;
+            }
         }
-        return;
     } else {
-    constexpr int G = SH / 4;        // 4-row groups per code row
-    constexpr int PL = R / 4;        // planes per lane
-    for(int c = threadIdx.x; c < kAlpha * G; c += blockDim.x) {
-        const int b = c / G, rg = c - b * G;
-        const uint32_t va = __ldg(reinterpret_cast<const uint32_t *>(g1 + (size_t) b * lp1 + i0) + rg);
-        const int ln = rg / PL, pl = rg - ln * PL;
-        uint4 o;
-        if constexpr(kNarrow) {
-            uint32_t vb = 0;
-            if((uint32_t) (i0 + 4 * rg) < lp2) vb = __ldg(reinterpret_cast<const uint32_t *>(g2 + (size_t) b * lp2 + i0) + rg);
-            o.x = __vadd2(sbyte2<0>(va, vb), gg);
-            o.y = __vadd2(sbyte2<1>(va, vb), gg);
-            o.z = __vadd2(sbyte2<2>(va, vb), gg);
-            o.w = __vadd2(sbyte2<3>(va, vb), gg);
-        } else {
+        static_assert(R % 4 == 0, "32-bit lanes use full planes");
+        constexpr int G = 8 * R;         // 4-row groups per code row
+        constexpr int PL = R / 4;        // planes per lane
+        for(int c = threadIdx.x; c < kAlpha * G; c += blockDim.x) {
+            const int b = c / G, rg = c - b * G;
+            const uint32_t va = __ldg(reinterpret_cast<const uint32_t *>(g1 + (size_t) b * lp1 + i0) + rg);
+            const int ln = rg / PL, pl = rg - ln * PL;
+            uint4 o;
             o.x = (uint32_t) sbyte<0>(va);
             o.y = (uint32_t) sbyte<1>(va);
             o.z = (uint32_t) sbyte<2>(va);
             o.w = (uint32_t) sbyte<3>(va);
+            *reinterpret_cast<uint4 *>(sprof + b * SH + pl * 128 + ln * 4) = o;
         }
-        *reinterpret_cast<uint4 *>(sprof + b * SH + pl * 128 + ln * 4) = o;
-    }
     }
 }
 
@@ -486,8 +515,9 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
                                             bool store_bound, int32_t g, int lane, typename K::W (&H)[R])
 {
     using W = typename K::W;
-    constexpr int SH = 32 * R;
     constexpr bool kB = std::is_same<K, Narrow>::value;
+    using L = Layout<R, kB>;
+    constexpr int SH = L::SH;
     const W ng = K::splat(-g);
     W diag;
     if constexpr(kB) {
@@ -502,8 +532,8 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
     W hlast = H[R - 1];
     uint32_t bq_cur = bound[lane], bq_nxt = bound[32 + lane];
     const uint32_t *prow = sprof + lane * 4;
-    constexpr int P = R / 4;                      // full profile planes per lane
-    const int half_off = P * 128 - lane * 2;      // half plane (R % 4 == 2) from prow
+    const int half_off = L::HALF - lane * 2;      // the 16-bit half plane, from prow
+    const int phalf_off = L::PHALF - lane * 2;    // the packed half plane, from prow
     const bool st31 = store_bound && lane == 31;
     int j = -lane;
     uint32_t cur = cols[j], nxt = cols[j + 1];   // columns -32..ncols+35 lie in the padded store
@@ -522,8 +552,8 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
             if(!kG || (unsigned) j < (unsigned) ncols) {
                 const uint32_t *pb = prow + cur * SH;
                 W sc[4];
-                auto load_plane = [&](int q) {
-                    if(q < P) {
+                auto load_plane = [&](int q) {   // 16-bit plane q (q == P16: the half plane)
+                    if(q < L::P16) {
                         const uint4 v = *reinterpret_cast<const uint4 *>(pb + q * 128);
                         sc[0] = (W) v.x; sc[1] = (W) v.y; sc[2] = (W) v.z; sc[3] = (W) v.w;
                     } else {
@@ -535,10 +565,29 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
                 if constexpr(kB) {
                     // T = max(T_left, T_up, T_diag + s + 2g); see Narrow.
                     W above = up, dprev = diag;
+                    uint4 pk;
 #pragma unroll
                     for(int r = 0; r < R; ++r) {
-                        if(r > 0 && (r & 3) == 0) load_plane(r >> 2);
-                        const W D = __vadd2(dprev, sc[r & 3]);
+                        W sr;
+                        if(r < L::R16) {
+                            if(r > 0 && (r & 3) == 0) load_plane(r >> 2);
+                            sr = sc[r & 3];
+                        } else {
+                            const int rr = r - L::R16;
+                            if((rr & 7) == 0) {
+                                if((rr >> 3) < L::P8) {
+                                    pk = *reinterpret_cast<const uint4 *>(pb + L::PACK + (rr >> 3) * 128);
+                                } else {
+                                    const uint2 v = *reinterpret_cast<const uint2 *>(pb + phalf_off);
+                                    pk.x = v.x;
+                                    pk.y = v.y;
+                                }
+                            }
+                            const int wi = (rr >> 1) & 3;
+                            const uint32_t w = wi == 0 ? pk.x : wi == 1 ? pk.y : wi == 2 ? pk.z : pk.w;
+                            sr = (rr & 1) ? prmt0<0x4341>(w) : prmt0<0x4240>(w);
+                        }
+                        const W D = __vadd2(dprev, sr);
                         dprev = H[r];
                         H[r] = __vimax3_u16x2(H[r], above, D);
                         above = H[r];
@@ -862,6 +911,7 @@ static inline bool narrow_ok(int64_t rows_p, int64_t cols, const ExtTable &t)
     const int64_t g2 = 2 * (int64_t) t.penalty;
     if((int64_t) t.letter_neg > g2) return false;
     const int64_t step = std::max<int64_t>((int64_t) t.letter_pos + g2, 0);
+    if(step > 0xff) return false;   // s + 2g is staged as a byte in packed rows
     return step * std::min(rows_p, cols) <= 0xffff;
 }
 
