@@ -9,10 +9,16 @@
 //   * the launch thread issues one merged persistent kernel per quantum,
 //     whose task list takes column groups from every admitted job, so work of
 //     a job that arrived while others were running shares the launch with
-//     them; two launches are kept in flight, and after each one the jobs whose
-//     last task ran are finished (scores copied out, device memory returned).
+//     them; two launches are kept in flight on two streams (each with its own
+//     boundary rows and task tables, so the second fills the SMs the first
+//     one's last tasks leave idle), and after each one the jobs whose last
+//     task ran are finished (scores copied out, device memory returned).
 // Job memory comes from a memory pool of the server in stream order, so
-// neither admission nor release waits for the launches in flight.
+// neither admission nor release waits for the launches in flight. The launch
+// thread returns memory on a stream of its own: the admission stream may be
+// capturing a CUDA graph, which would absorb a release enqueued there.
+// msa_serve_start pays the one-time costs (pool growth, launch buffers, pinned
+// staging, a first launch on no work) before the server takes jobs.
 //
 // Two policies share the quantum's cell budget among the admitted jobs:
 //   * continuous (batch_window_us = 0): every job gets an equal share, so a
