@@ -285,3 +285,26 @@ def test_16bit_lanes_near_their_bound(gpu, golden, mode):
         assert np.array_equal(got, want), (lc, got, want)
         if mode == _lib.MSA_NW_PERSISTENT:
             assert (pairwise.last_stats().narrow_tasks > 0) == narrow, lc
+
+
+@pytest.mark.parametrize("mode", MODES)
+def test_packed_profile_rows_at_their_byte_bound(gpu, mode):
+    # Packed profile rows hold s + 2g in one byte. Match +1, mismatch -2 and
+    # gap 127 make s + 2g reach 255 on matches, and the 257 columns of the
+    # second sequence put T at 257 * 255 = 0xffff: the batched kernel must
+    # still take 16-bit lanes (the 600-row strip has R = 20, so some of its
+    # rows are packed). Gap 128 pushes s + 2g past a byte: 32-bit lanes.
+    m = np.full((25, 25), -2, np.int32)
+    np.fill_diagonal(m, 1)
+    la, lc, lm = 600, 257, 250
+    seqs = [b"A" * la, b"A" * lc, b"C" * lm]
+    wl = W.Workload("edge", [np.frombuffer(s, np.uint8) for s in seqs], "default", 0)
+    flat, offs, lens = wl.flat_units()
+    for g, narrow in ((127, True), (128, False)):
+        got = pairwise.score_units(flat, offs, lens, ScoringTable.custom(m, g), mode)
+        # (1,0): lc matches and la - lc gaps; (2,0) and (2,1): every C against
+        # an A (a mismatch costs less than two gaps), the rest gaps.
+        want = np.array([lc - g * (la - lc), -2 * lm - g * (la - lm), -2 * lm - g * (lc - lm)], np.int32)
+        assert np.array_equal(got, want), (g, got, want)
+        if mode == _lib.MSA_NW_PERSISTENT:
+            assert (pairwise.last_stats().narrow_tasks > 0) == narrow, g
