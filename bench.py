@@ -671,30 +671,42 @@ def main():
         props = torch.cuda.get_device_properties(local)
         sm_mhz = clocks.get("sm_mhz") or 1965.0
         nsm = props.multi_processor_count
+        # DRAM traffic and counted instructions per cell of this kernel on this
+        # workload, from the committed ncu summaries.
+        traffic = inst_per_cell = None
+        tp = ROOT / "profiles" / "nw_traffic.json"
+        if tp.exists():
+            try:
+                tj = json.loads(tp.read_text())
+                traffic = tj.get(args.workload)
+                inst_per_cell = tj.get(args.workload + "_inst_per_cell")
+            except Exception:
+                traffic = inst_per_cell = None
         # Ceilings of the batched kernel from rates measured here per SM clock
         # (msa_probe_op). A cell reads its score from shared memory: 2 bytes in
         # a 16-bit profile row, 1 byte in a packed row (a share f of the cells,
         # from the kernel's plan), so 2 - f bytes per cell. The ALU pipe
         # (64 lanes/clk/SM) carries one vimax3 per two cells and one PRMT per
-        # two cells of a packed row: (1 + f) / 2 lane-ops per cell. The lower
-        # of the two is the roofline.
+        # two cells of a packed row: (1 + f) / 2 lane-ops per cell. The lowest
+        # ceiling (these two, and issue below) is the roofline.
         lds = probe_rate(ctx, 15)
         cell_ops = probe_rate(ctx, 14)
         f_packed = packed_row_fraction(wl)
         smem_peak = nsm * (lds / (2.0 - f_packed)) * sm_mhz * 1e6 / 1e9
         alu_peak = nsm * (64.0 / ((1.0 + f_packed) / 2.0)) * sm_mhz * 1e6 / 1e9
         cell_peak = nsm * (2.0 * cell_ops) * sm_mhz * 1e6 / 1e9
-        roof = min(smem_peak, alu_peak)
+        # Issue: 4 warp-instructions (128 lane-instructions) per SM per clock
+        # over the lane-instructions per cell that ncu counted for this kernel
+        # on this workload (profiles/nw_traffic.json), when there is a count.
+        issue_peak = nsm * (128.0 / inst_per_cell) * sm_mhz * 1e6 / 1e9 if inst_per_cell else None
+        ceilings = {"smem": smem_peak, "alu": alu_peak}
+        if issue_peak:
+            ceilings["issue"] = issue_peak
+        bound = min(ceilings, key=ceilings.get)
+        roof = ceilings[bound]
         # The four-op int32 issue figure (two max operations per cell on the ALU
         # pipe, 64 lanes/clk/SM): 32 cells/clk/SM.
         peak = nsm * 64 * sm_mhz * 1e6 / 2 / 1e9
-        traffic = None
-        tp = ROOT / "profiles" / "nw_traffic.json"
-        if tp.exists():
-            try:
-                traffic = json.loads(tp.read_text()).get(args.workload)
-            except Exception:
-                traffic = None
         cpu = None
         if not args.no_cpu:
             cpu = run_cpu_reference(wl, 1, 0, args.cpu_cells)
@@ -711,18 +723,21 @@ def main():
                     "h2d_bytes_per_step": int(flat.nbytes + offs.nbytes + lens.nbytes),
                     "d2h_bytes_per_step": int(npairs * 4), "scores_match": e2e_ok},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "smem" if smem_peak <= alu_peak else "alu", "achieved": kernel_gcups,
+            "roofline": {"bound": bound, "achieved": kernel_gcups,
                          "peak": roof, "unit": "GCUPS", "frac": kernel_gcups / roof, "traffic": traffic,
                          "frac_int32_issue": kernel_gcups / peak,
-                         "packed_row_fraction": f_packed,
+                         "packed_row_fraction": f_packed, "inst_per_cell_counted": inst_per_cell,
                          "ceilings_gcups": {"smem_profile_reads": smem_peak, "alu_pipe": alu_peak,
+                                            "issue_counted_instructions": issue_peak,
                                             "cell_ops_16x2_probe": cell_peak, "int32_issue_4ops_per_cell": peak},
                          "measured_per_sm_clk": {"lds_bytes": lds, "cell_16x2_lane_ops": cell_ops},
                          "peak_basis": f"min of {nsm} SM x {lds:.1f} shared-memory bytes/clk (measured, "
-                                       f"ld.shared.v4) / (2 - {f_packed:.3f}) bytes of profile per cell and "
-                                       f"{nsm} SM x 64 ALU lanes/clk / ((1 + {f_packed:.3f}) / 2) lane-ops per cell, "
-                                       f"x {sm_mhz:.0f} MHz (median sampled); frac_int32_issue is against "
-                                       f"{nsm} SM x 64 ALU lanes/clk / 2 max-ops per cell"},
+                                       f"ld.shared.v4) / (2 - {f_packed:.3f}) bytes of profile per cell, "
+                                       f"{nsm} SM x 64 ALU lanes/clk / ((1 + {f_packed:.3f}) / 2) lane-ops per cell"
+                                       + (f" and {nsm} SM x 128 issued lane-instructions/clk / {inst_per_cell} "
+                                          f"counted per cell" if inst_per_cell else "")
+                                       + f", x {sm_mhz:.0f} MHz (median sampled); frac_int32_issue is against "
+                                         f"{nsm} SM x 64 ALU lanes/clk / 2 max-ops per cell"},
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
