@@ -9,15 +9,17 @@
 // exactly.
 //
 // Work layout: one warp runs one task. A task is one (rows, cols) pair, or on
-// the 16-bit path two pairs sharing the rows sequence, one per 16-bit half.
-// Lane k owns R consecutive rows of a 32*R-row strip and sweeps the columns one
-// step behind lane k-1: the cell above its first row arrives from lane k-1 by
-// __shfl_up_sync, so a strip advances one anti-diagonal per step with no
-// block-wide barrier. Strips of a long rows sequence are chained through a
-// per-warp boundary row in global memory. Substitution scores come from a
-// per-sequence score profile (one int8 row per residue code) staged per strip
-// in shared memory, laid out [code][lane][R] so that the 16-byte profile loads
-// of a warp are bank-conflict free whatever codes the lanes hold.
+// the 16-bit path two pairs sharing the column sequence (the two rows
+// sequences of a rows pair, one per 16-bit half). Lane k owns R consecutive
+// rows of a 32*R-row strip and sweeps the columns one step behind lane k-1:
+// the cell above its first row arrives from lane k-1 by __shfl_up_sync, so a
+// strip advances one anti-diagonal per step with no block-wide barrier. Strips
+// of a long rows sequence are chained through a per-warp boundary row in
+// global memory. Substitution scores come from a per-sequence score profile
+// (one int8 row per residue code) staged per strip in shared memory, in planes
+// whose 16-byte (or 8-byte) loads are bank-conflict free whatever codes the
+// lanes hold; the batched kernel keeps part of each strip as packed bytes
+// (Layout) to halve those rows' shared-memory traffic.
 #include <cstdio>
 #include <algorithm>
 #include <cmath>
