@@ -138,10 +138,22 @@ def run_cpu_reference(wl, steps: int, warmup: int, target_cells: float):
             times.append(dt)
             cells_all.append(cells)
     gcups = sum(cells_all) / sum(times) / 1e9
-    return {"value": gcups, "unit": "GCUPS", "cores": threads, "kind": "reference",
+    return {"value": gcups, "unit": "GCUPS", "cores": threads, "kind": "reference", "cpu": cpu_model(),
             "sample": f"{len(times)} x ~{target_cells:.2g}-cell uniform pair samples of the workload, "
                       f"Museqa needleman::sequential (oracle/_ref) on {threads} host threads",
             "seconds": sum(times)}
+
+
+def cpu_model() -> str:
+    """The host CPU's model name (/proc/cpuinfo), or the platform's processor string."""
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
 
 
 def reference_arm(args):
