@@ -54,8 +54,6 @@ __device__ __forceinline__ uint32_t sbyte2(uint32_t lo, uint32_t hi)
 }
 
 __device__ __forceinline__ uint32_t dup16(int32_t v) { return ((uint32_t) v & 0xffffu) | ((uint32_t) v << 16); }
-__device__ __forceinline__ int32_t lo16(uint32_t v) { return (int32_t) (int16_t) (v & 0xffffu); }
-__device__ __forceinline__ int32_t hi16(uint32_t v) { return (int32_t) (int16_t) (v >> 16); }
 
 // One cell: max(up - g, max(left - g, diag + s)). The inner max depends only on
 // the previous column, so the serial chain down a lane's rows is one DPX op.
@@ -141,11 +139,11 @@ __device__ __forceinline__ void stage_profile(int8_t *sprof, const int8_t *__res
     }
 }
 
-// Runs one task on the calling warp. Column sweep: ncolsA columns of colsA in
-// the low half (or the whole word), ncolsB <= ncolsA columns of colsB in the
-// high half (Narrow only). kSkip: END units in the columns copy the left
-// neighbour (sequential.cpp:53-60) instead of scoring.
-// Returns H[nrows][ncolsA] (resA) and H[nrows][ncolsB] (resB).
+// Runs one task in 32-bit lanes on the calling warp (the plain and the
+// reference-orientation kernels): ncolsA columns of colsA against nrows rows.
+// kSkip: END units in the columns copy the left neighbour
+// (sequential.cpp:53-60) instead of scoring. Returns H[nrows][ncolsA] (resA);
+// colsB, ncolsB and resB are unused (resB = 0).
 template <int R, class K, bool kSkip>
 __device__ __forceinline__ void run_task(const int8_t *__restrict__ gprof, uint32_t lp, int nrows,
                                          const uint8_t *__restrict__ colsA, int ncolsA,
@@ -153,9 +151,9 @@ __device__ __forceinline__ void run_task(const int8_t *__restrict__ gprof, uint3
                                          int8_t *sprof, uint32_t *__restrict__ bound,
                                          int32_t g, int lane, int32_t &resA, int32_t &resB)
 {
+    static_assert(std::is_same<K, Wide>::value, "run_task sweeps 32-bit lanes");
     using W = typename K::W;
     constexpr int SH = 32 * R;
-    constexpr bool kNarrow = std::is_same<K, Narrow>::value;
     const int nstrips = (nrows + SH - 1) / SH;
     const W ng = K::splat(-g);
     int32_t outA = 0, outB = 0;
@@ -187,8 +185,6 @@ __device__ __forceinline__ void run_task(const int8_t *__restrict__ gprof, uint3
         }
         int clampA = ncolsA - 1;
         uint32_t curA = colsA[min(max(-lane, 0), clampA)];
-        uint32_t curB = 0;
-        if constexpr(kNarrow) curB = colsB[min(max(-lane, 0), ncolsB - 1)];
 
         const int tend = ncolsA + klast;
         for(int t = 0; t < tend; ++t) {
@@ -206,76 +202,41 @@ __device__ __forceinline__ void run_task(const int8_t *__restrict__ gprof, uint3
             const int j = t - lane;
             const int jn = min(max(j + 1, 0), clampA);
             const uint32_t nxtA = colsA[jn];
-            uint32_t nxtB = 0;
-            if constexpr(kNarrow) nxtB = colsB[min(jn, ncolsB - 1)];
 
             if(j >= 0 && j < ncolsA) {
                 const bool skip = kSkip && curA == (uint32_t) kEnd;
                 if(!skip) {
                     ProfWords<R> pa;
                     pa.load(sprof, (int) curA, lane);
-                    if constexpr(kNarrow) {
-                        ProfWords<R> pb;
-                        pb.load(sprof, (int) curB, lane);
-                        W d = diag, u = up;
+                    W d = diag, u = up;
 #pragma unroll
-                        for(int q = 0; q < R / 4; ++q) {
+                    for(int q = 0; q < R / 4; ++q) {
 #pragma unroll
-                            for(int k = 0; k < 4; ++k) {
-                                const int r = 4 * q + k;
-                                W sc;
-                                if(k == 0) sc = sbyte2<0>(pa.w[q], pb.w[q]);
-                                else if(k == 1) sc = sbyte2<1>(pa.w[q], pb.w[q]);
-                                else if(k == 2) sc = sbyte2<2>(pa.w[q], pb.w[q]);
-                                else sc = sbyte2<3>(pa.w[q], pb.w[q]);
-                                const W h = K::cell(d, sc, H[r], u, ng);
-                                d = H[r];
-                                H[r] = h;
-                                u = h;
-                            }
-                        }
-                    } else {
-                        W d = diag, u = up;
-#pragma unroll
-                        for(int q = 0; q < R / 4; ++q) {
-#pragma unroll
-                            for(int k = 0; k < 4; ++k) {
-                                const int r = 4 * q + k;
-                                W sc;
-                                if(k == 0) sc = sbyte<0>(pa.w[q]);
-                                else if(k == 1) sc = sbyte<1>(pa.w[q]);
-                                else if(k == 2) sc = sbyte<2>(pa.w[q]);
-                                else sc = sbyte<3>(pa.w[q]);
-                                const W h = K::cell(d, sc, H[r], u, ng);
-                                d = H[r];
-                                H[r] = h;
-                                u = h;
-                            }
+                        for(int k = 0; k < 4; ++k) {
+                            const int r = 4 * q + k;
+                            W sc;
+                            if(k == 0) sc = sbyte<0>(pa.w[q]);
+                            else if(k == 1) sc = sbyte<1>(pa.w[q]);
+                            else if(k == 2) sc = sbyte<2>(pa.w[q]);
+                            else sc = sbyte<3>(pa.w[q]);
+                            const W h = K::cell(d, sc, H[r], u, ng);
+                            d = H[r];
+                            H[r] = h;
+                            u = h;
                         }
                     }
                 }
                 hlast = H[R - 1];
                 if(!last && lane == 31) bound[j] = (uint32_t) hlast;
-                if(last && lane == klast) {
-                    if(j == ncolsA - 1) {
-                        W v = H[0];
+                if(last && lane == klast && j == ncolsA - 1) {
+                    W v = H[0];
 #pragma unroll
-                        for(int r = 1; r < R; ++r) if(r == rlast) v = H[r];
-                        if constexpr(kNarrow) outA = lo16(v); else outA = (int32_t) v;
-                    }
-                    if constexpr(kNarrow) {
-                        if(j == ncolsB - 1) {
-                            W v = H[0];
-#pragma unroll
-                            for(int r = 1; r < R; ++r) if(r == rlast) v = H[r];
-                            outB = hi16(v);
-                        }
-                    }
+                    for(int r = 1; r < R; ++r) if(r == rlast) v = H[r];
+                    outA = (int32_t) v;
                 }
                 diag = up;
             }
             curA = nxtA;
-            if constexpr(kNarrow) curB = nxtB;
         }
         if(last) {
             resA = __shfl_sync(kFull, outA, klast);
