@@ -197,3 +197,30 @@ def test_encode_blocks_abi_matches_reference(ref, text):
     _lib.check(_lib.lib().msa_encode_blocks(text, len(text), out.ctypes.data_as(ctypes.POINTER(ctypes.c_uint16))))
     want = O.ref_encode_blocks(text)
     assert np.array_equal(out[:len(want)], want)
+
+
+def test_bench_packed_row_fraction_replays_the_strip_plan():
+    """bench.py's roofline weighs the batched kernel's packed profile rows by
+    replaying its plan; check the replay against a pair-by-pair count on a
+    small uneven workload (rows pairs of the length-sorted sequences, strips of
+    32R rows with R even and at most 32, 8 floor(R/16) packed rows per lane)."""
+    import sys
+    root = Path(__file__).resolve().parents[1]
+    if str(root) not in sys.path:
+        sys.path.insert(0, str(root))
+    import bench
+    wl = W.random_set(90, 41, 20, 3000, alphabet=b"ACGT")
+    e = np.sort(wl.lengths().astype(np.int64))[::-1]
+    packed = total = 0.0
+    for k in range((len(e) + 1) // 2):
+        a1, a2 = 2 * k, min(2 * k + 1, len(e) - 1)
+        nst = -(-int(e[a1]) // 1024)
+        r = -(-int(e[a1]) // (32 * nst))
+        r += r % 2
+        for b in range(2 * k + 1, len(e)):
+            for a in {a1, a2}:
+                cells = float(e[a] * e[b])
+                packed += cells * (8 * (r // 16)) / r
+                total += cells
+    assert bench.packed_row_fraction(wl) == pytest.approx(packed / total, rel=1e-12)
+    assert 0.0 <= packed / total <= 0.5
