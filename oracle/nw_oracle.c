@@ -106,6 +106,15 @@ int oracle_nj(int64_t n, const float *tri,
               float *distance, uint32_t *level,
               uint32_t *join_x, uint32_t *join_y)
 {
+    return oracle_nj_order(n, tri, ORACLE_NJ_SYMMETRIC, parent, child0, child1, distance, level, join_x, join_y);
+}
+
+int oracle_nj_order(int64_t n, const float *tri, int order,
+                    uint32_t *parent, uint32_t *child0, uint32_t *child1,
+                    float *distance, uint32_t *level,
+                    uint32_t *join_x, uint32_t *join_y)
+{
+    if(order != ORACLE_NJ_SYMMETRIC && order != ORACLE_NJ_LINEAR) return -1;
     if(n < 2) return 0;
     const int64_t nodes = 2 * n - 1;
 
@@ -206,12 +215,21 @@ int oracle_nj(int64_t n, const float *tri,
         S[px] = new_sum;
         map[px] = next_parent;
 
-        /* update_cache, symmetric (sequential.cpp:210-224): swap logical 0 and
-         * y, then drop logical 0; every later index moves down by one. */
-        {
+        if(order == ORACLE_NJ_SYMMETRIC) {
+            /* update_cache, symmetric (sequential.cpp:210-224): swap logical 0
+             * and y, then drop logical 0; every later index moves down by one. */
             const int64_t p0 = perm[0];
             for(int64_t k = 0; k + 1 < c; ++k) perm[k] = perm[k + 1];
             if(by > 0) perm[by - 1] = p0;
+        } else {
+            /* update_cache, linear (sequential.cpp:189-203): swap y and the
+             * last logical index c-1 (matrix rows and columns, row sums and the
+             * OTU map: matrix.cu:443-460 exchanges every off-diagonal pair, the
+             * diagonal being zero), then drop the last; no index shifts. The
+             * new node itself moves into y when x was the last. */
+            const int64_t py2 = perm[by];
+            perm[by] = perm[c - 1];
+            perm[c - 1] = py2;
         }
 
         ++next_parent;

@@ -64,6 +64,20 @@ int oracle_nj(int64_t n, const float *tri,
               float *distance, uint32_t *level,
               uint32_t *join_x, uint32_t *join_y);
 
+/*
+ * The same with the removal order chosen: ORACLE_NJ_SYMMETRIC as above, or
+ * ORACLE_NJ_LINEAR for njoining::sequential<transform::linear<2>>
+ * (sequential.cpp:189-203, 356-358): the removed OTU y trades places with the
+ * last logical OTU, which is then dropped, so no other index moves. Returns
+ * -1 for an unknown order.
+ */
+#define ORACLE_NJ_SYMMETRIC 0
+#define ORACLE_NJ_LINEAR 1
+int oracle_nj_order(int64_t n, const float *tri, int order,
+                    uint32_t *parent, uint32_t *child0, uint32_t *child1,
+                    float *distance, uint32_t *level,
+                    uint32_t *join_x, uint32_t *join_y);
+
 #ifdef __cplusplus
 }
 #endif

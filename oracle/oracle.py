@@ -17,8 +17,14 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
+# The reference project's root (its src/, test/ and db/ directories), present
+# only where the checker libraries are built; MSA_REFERENCE overrides it.
+REFERENCE_ROOT = Path(os.environ.get("MSA_REFERENCE", "/root/reference"))
 RESTATEMENT = HERE / "liboracle.so"
 REFERENCE = HERE / "_ref" / "libmuseqa_ref.so"
+# The reference-side binding of libmsa_b200.so (ref_b200.cpp): Museqa's own
+# algorithm interfaces implemented over the C ABI, linked with the reference.
+BINDING = HERE / "_ref" / "libmuseqa_b200.so"
 
 _vp = ctypes.c_void_p
 
@@ -54,6 +60,50 @@ def reference():
     return _ref
 
 
+_bind = None
+
+
+def binding():
+    """The reference-side binding library, or None when it was not built."""
+    global _bind
+    if _bind is None:
+        if reference() is None:
+            return None
+        _bind = _load(BINDING)
+        if _bind is not None:
+            _bind.b200_ref_last_error.restype = ctypes.c_char_p
+            _bind.b200_ref_nw_all_pairs.argtypes = [ctypes.c_int, _vp, _vp, ctypes.c_char_p, _vp, _vp]
+            _bind.b200_ref_nj.argtypes = [ctypes.c_int, _vp, ctypes.c_int, ctypes.c_char_p, _vp, _vp]
+    return _bind
+
+
+def binding_nw_all_pairs(seqs: list, table: str):
+    """(scores of the needleman_b200 algorithm object, scores of
+    pairwise::run(db, table, "sequential")) on the same reference database."""
+    lib = binding()
+    n = len(seqs)
+    arr, lens = _cstrs(seqs)
+    a = np.zeros(n * (n - 1) // 2, np.float32)
+    b = np.zeros(n * (n - 1) // 2, np.float32)
+    if lib.b200_ref_nw_all_pairs(n, ctypes.cast(arr, _vp), _ptr(lens), table.encode(), _ptr(a), _ptr(b)):
+        raise RuntimeError(lib.b200_ref_last_error().decode())
+    return a, b
+
+
+def binding_nj(tri: np.ndarray, n: int, linear: bool, ref_name: str):
+    """(tree of the njoining_b200 algorithm object, tree of
+    phylogeny::run(matrix, n, ref_name)), each as 2n-1 rows of (parent,
+    child0, child1, distance bits, level)."""
+    lib = binding()
+    tri = np.ascontiguousarray(tri, np.float32)
+    m = max(2 * n - 1, 1)
+    a = np.zeros((m, 5), np.uint32)
+    b = np.zeros((m, 5), np.uint32)
+    if lib.b200_ref_nj(n, _ptr(tri), int(linear), ref_name.encode(), _ptr(a), _ptr(b)):
+        raise RuntimeError(lib.b200_ref_last_error().decode())
+    return a, b
+
+
 def restatement():
     global _res
     if _res is None:
@@ -64,6 +114,7 @@ def restatement():
             _res.oracle_nw_all_pairs.argtypes = [ctypes.c_int64, _vp, _vp, _vp, _vp, ctypes.c_int, ctypes.c_int,
                                                  ctypes.c_int32, _vp]
             _res.oracle_nj.argtypes = [ctypes.c_int64, _vp] + [_vp] * 7
+            _res.oracle_nj_order.argtypes = [ctypes.c_int64, _vp, ctypes.c_int] + [_vp] * 7
             _res.oracle_encode_char.argtypes = [ctypes.c_char]
             _res.oracle_encode_char.restype = ctypes.c_uint8
     return _res
@@ -180,7 +231,12 @@ def oracle_nw_all_pairs(units: np.ndarray, offs: np.ndarray, lens: np.ndarray, t
     return out
 
 
-def oracle_nj(tri: np.ndarray, n: int) -> dict:
+NJ_ORDER = {"symmetric": 0, "linear": 1}
+
+
+def oracle_nj(tri: np.ndarray, n: int, order: str = "symmetric") -> dict:
+    """The restated NJ; `order` is the removal order: "symmetric"
+    (sequential_symmetric) or "linear" (sequential_linear)."""
     lib = restatement()
     tri = np.ascontiguousarray(tri, np.float32)
     m = max(2 * n - 1, 1)
@@ -188,7 +244,8 @@ def oracle_nj(tri: np.ndarray, n: int) -> dict:
     D = np.zeros(m, np.float32)
     jx = np.zeros(max(n - 1, 1), np.uint32)
     jy = np.zeros(max(n - 1, 1), np.uint32)
-    rc = lib.oracle_nj(n, _ptr(tri), _ptr(P), _ptr(C0), _ptr(C1), _ptr(D), _ptr(L), _ptr(jx), _ptr(jy))
+    rc = lib.oracle_nj_order(n, _ptr(tri), NJ_ORDER[order], _ptr(P), _ptr(C0), _ptr(C1), _ptr(D), _ptr(L),
+                             _ptr(jx), _ptr(jy))
     if rc:
         raise RuntimeError(f"oracle_nj failed ({rc})")
     return {"parent": P, "child0": C0, "child1": C1, "distance": D, "level": L}

@@ -29,8 +29,11 @@ def built_library():
     build.build()
     import subprocess
     subprocess.run(["make", "-s", "-C", str(ROOT / "oracle")], check=True)
-    if Path("/root/reference/src").is_dir() and not (ROOT / "oracle/_ref/libmuseqa_ref.so").exists():
-        subprocess.run(["make", "-s", "-j8", "-C", str(ROOT / "oracle"), "ref"], check=True)
+    from oracle.oracle import REFERENCE_ROOT
+    built = all((ROOT / "oracle/_ref" / f).exists() for f in ("libmuseqa_ref.so", "libmuseqa_b200.so"))
+    if (REFERENCE_ROOT / "src").is_dir() and not built:
+        subprocess.run(["make", "-s", "-j8", "-C", str(ROOT / "oracle"), "ref",
+                        f"MSA_REFERENCE={REFERENCE_ROOT}"], check=True)
     yield
 
 

@@ -2,12 +2,14 @@
 CPU implementation (oracle/_ref/libmuseqa_ref.so, built from the reference
 sources by `make -C oracle ref`).
 
-    python tests/golden/make_golden.py [--c4]
+    python tests/golden/make_golden.py [--c4 | --c4-tri FILE.npy]
 
 Inputs are the seeded synthetic workloads of msa_b200.workloads; outputs are
 the reference's float scores (stored as int32, they are integers) and trees.
 --c4 also scores the full 2,000-sequence c4 set (about 1e12 cells; minutes
-on all host cores) and builds its 2,000-taxon tree.
+on all host cores) and builds its 2,000-taxon trees (symmetric and linear
+removal orders). --c4-tri rebuilds only the trees, from a saved int32
+triangle that must hash to the recorded reference matrix.
 """
 from __future__ import annotations
 
@@ -79,7 +81,7 @@ def main() -> None:
         sys.exit("build the reference first: make -C oracle ref")
     t0 = time.time()
     gold = {"generator": "tests/golden/make_golden.py", "reference": "Museqa v0.1.1 needleman::sequential, "
-            "njoining::sequential_symmetric (oracle/_ref)"}
+            "njoining::sequential_symmetric and sequential_linear (oracle/_ref)"}
 
     order = ["default", "blosum62", "blosum45", "blosum50", "blosum80", "blosum90", "pam250"]
     gold["tables"] = []
@@ -93,7 +95,8 @@ def main() -> None:
     c1 = W.c1()
     tri = full_set(c1, "blosum62")
     gold["c1"] = {"seed": 1, "table": "blosum62", "scores": tri.tolist(),
-                  "tree": tree_dict(O.ref_nj(tri.astype(np.float32), c1.n))}
+                  "tree": tree_dict(O.ref_nj(tri.astype(np.float32), c1.n)),
+                  "tree_linear": tree_dict(O.ref_nj(tri.astype(np.float32), c1.n, "njoining-sequential-linear"))}
     gold["edge"] = edge_sets()
 
     # Sampled pairs of the large configurations.
@@ -112,6 +115,8 @@ def main() -> None:
     print(f"golden.json written in {time.time() - t0:.1f}s")
 
     if "--c4" in sys.argv:
+        # The c4 matrix scored by the reference (about 17 minutes on 8 host
+        # threads), then its two guide trees.
         wl = W.c4()
         n = wl.n
         ii, jj = np.tril_indices(n, -1)
@@ -121,13 +126,32 @@ def main() -> None:
         sc = O.ref_nw_pairs(wl.strings(), ii, jj, "blosum62", threads=os.cpu_count() or 1)
         tri = sc.astype(np.int32)
         t2 = time.time()
-        tree = O.ref_nj(sc, n)
-        t3 = time.time()
-        c4 = {"n": n, "table": "blosum62", "scores_sha256": tri_sha(tri), "tree": tree_dict(tree),
-              "nw_seconds": t2 - t1, "nj_seconds": t3 - t2, "threads": os.cpu_count()}
-        (OUT / "golden_c4.json").write_text(json.dumps(c4))
-        np.save(OUT.parent.parent / "_work" / "c4_tri.npy", tri)
-        print(f"golden_c4.json: NW {t2 - t1:.1f}s, NJ {t3 - t2:.2f}s")
+        c4 = {"n": n, "table": "blosum62", "scores_sha256": tri_sha(tri), "nw_seconds": t2 - t1,
+              "threads": os.cpu_count()}
+        c4_trees(c4, tri)
+        print(f"golden_c4.json: NW {t2 - t1:.1f}s, NJ {c4['nj_seconds']:.2f}s")
+    elif "--c4-tri" in sys.argv:
+        # The c4 trees only, from a saved int32 triangle (.npy) whose SHA-256
+        # must equal the one recorded when the reference scored c4, so the
+        # trees are the reference's on the reference's own matrix.
+        path = sys.argv[sys.argv.index("--c4-tri") + 1]
+        tri = np.load(path).astype(np.int32)
+        c4 = json.loads((OUT / "golden_c4.json").read_text())
+        if tri_sha(tri) != c4["scores_sha256"]:
+            raise SystemExit(f"{path} is not the reference's c4 matrix (SHA-256 differs)")
+        c4_trees(c4, tri)
+        print(f"golden_c4.json trees rewritten, NJ {c4['nj_seconds']:.2f}s")
+
+
+def c4_trees(c4: dict, tri: np.ndarray) -> None:
+    """Adds the reference's symmetric (`tree`) and linear (`tree_linear`)
+    guide trees of the c4 matrix to `c4` and writes golden_c4.json."""
+    n = c4["n"]
+    t0 = time.time()
+    c4["tree"] = tree_dict(O.ref_nj(tri.astype(np.float32), n))
+    c4["nj_seconds"] = time.time() - t0
+    c4["tree_linear"] = tree_dict(O.ref_nj(tri.astype(np.float32), n, "njoining-sequential-linear"))
+    (OUT / "golden_c4.json").write_text(json.dumps(c4))
 
 
 if __name__ == "__main__":

@@ -106,7 +106,8 @@ def test_fast_fasta_loader_equals_python(tmp_path):
 
 
 def test_fast_fasta_loader_on_the_reference_databases():
-    db_dir = Path("/root/reference/db")
+    from oracle.oracle import REFERENCE_ROOT
+    db_dir = REFERENCE_ROOT / "db"
     files = sorted(db_dir.glob("*.fasta")) if db_dir.is_dir() else []
     if not files:
         pytest.skip("the reference's FASTA databases are not present")

@@ -164,7 +164,8 @@ def test_fasta_unknown_file_raises():
 def test_reference_fixture_digests():
     # The reference's own loader test pins MD5s of decoded contents
     # (test/loader.py:16-34); check them where the reference tree is present.
-    fx = Path("/root/reference/test/fixtures")
+    from oracle.oracle import REFERENCE_ROOT
+    fx = REFERENCE_ROOT / "test" / "fixtures"
     if not fx.is_dir():
         pytest.skip("reference fixtures not present")
     db = Database.load(str(fx / "mock2.fasta"))
@@ -224,3 +225,13 @@ def test_bench_packed_row_fraction_replays_the_strip_plan():
                 total += cells
     assert bench.packed_row_fraction(wl) == pytest.approx(packed / total, rel=1e-12)
     assert 0.0 <= packed / total <= 0.5
+
+
+def test_phylogeny_names_select_the_reference_order():
+    """src/phylogeny/phylogeny.cpp:26-41: the linear transform for exactly four
+    names; an unknown name raises the reference's message."""
+    lin = {n for n in phylogeny.list() if phylogeny.order_of(n) == _lib.MSA_NJ_LINEAR}
+    assert lin == {"linear", "njoining-linear", "njoining-sequential-linear", "njoining-distributed-linear"}
+    assert len(phylogeny.list()) == 14
+    with pytest.raises(RuntimeError, match="unknown phylogeny algorithm 'nope'"):
+        phylogeny.order_of("nope")

@@ -88,6 +88,41 @@ def test_restatement_nj_matches_reference(ref, n, kind):
     assert np.array_equal(r["distance"].view(np.uint32), o["distance"].view(np.uint32))
 
 
+@pytest.mark.parametrize("n,kind", [(2, "ties"), (3, "ties"), (9, "ties"), (17, "ties"), (33, "ties"),
+                                    (60, "ties"), (120, "ties"), (60, "wide"), (150, "wide"), (300, "neg")])
+def test_restatement_nj_linear_matches_reference(ref, n, kind):
+    """The linear removal order (njoining-sequential-linear) against the
+    compiled reference; it differs from the symmetric order's tree on most of
+    these inputs, so the two orders are told apart."""
+    rng = np.random.default_rng(7000 + n)
+    m = n * (n - 1) // 2
+    tri = {"ties": rng.integers(-3, 4, m), "wide": rng.integers(-5000, 5000, m),
+           "neg": -rng.integers(0, 100, m)}[kind].astype(np.float32)
+    r = O.ref_nj(tri, n, "njoining-sequential-linear")
+    o = O.oracle_nj(tri, n, "linear")
+    for k in ("parent", "child0", "child1", "level"):
+        assert np.array_equal(r[k], o[k]), k
+    assert np.array_equal(r["distance"].view(np.uint32), o["distance"].view(np.uint32))
+
+
+def test_linear_and_symmetric_orders_differ(ref):
+    rng = np.random.default_rng(5)
+    n = 33
+    tri = rng.integers(-3, 4, n * (n - 1) // 2).astype(np.float32)
+    a = O.oracle_nj(tri, n, "linear")
+    b = O.oracle_nj(tri, n, "symmetric")
+    assert not (np.array_equal(a["parent"], b["parent"]) and
+                np.array_equal(a["distance"].view(np.uint32), b["distance"].view(np.uint32)))
+
+
 def test_reference_scores_are_exact_integers(golden):
     for e in golden["edge"]:
         assert all(isinstance(v, int) for v in e["scores"])
+
+
+def test_reference_binding_library_loads(ref):
+    """The reference-side binding (oracle/ref_b200.cpp) links against the
+    reference and libmsa_b200.so and exports its two test entry points."""
+    lib = O.binding()
+    assert lib is not None
+    assert hasattr(lib, "b200_ref_nw_all_pairs") and hasattr(lib, "b200_ref_nj")
