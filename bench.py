@@ -205,22 +205,38 @@ def nj_leg(lib, ctx, steps: int = 3, cpu: bool = True) -> dict:
     _lib.check(lib.msa_nw_all_pairs(ctx.handle, h.value, ctypes.byref(table._t), _lib.MSA_NW_PERSISTENT,
                                     ctypes.c_void_p(tri.data_ptr()), 1), ctx.handle)
     lib.msa_seqs_release(ctx.handle, h.value)
-    nodes = (_lib.MsaOtu * (2 * n - 1))()
-    kms, tms = [], []
-    for s in range(1 + steps):
-        _lib.check(lib.msa_nj(ctx.handle, ctypes.c_void_p(tri.data_ptr()), _lib.MSA_TRI_I32_DEVICE, n, nodes),
-                   ctx.handle)
-        st = _lib.MsaNjStats()
-        lib.msa_nj_last_stats(ctx.handle, ctypes.byref(st))
-        if s >= 1:
-            kms.append(st.kernel_ms)
-            tms.append(st.total_ms)
+    def run_nj(order):
+        nodes = (_lib.MsaOtu * (2 * n - 1))()
+        kms, tms = [], []
+        for s in range(1 + steps):
+            _lib.check(lib.msa_nj_order(ctx.handle, ctypes.c_void_p(tri.data_ptr()), _lib.MSA_TRI_I32_DEVICE, n,
+                                        order, nodes), ctx.handle)
+            st = _lib.MsaNjStats()
+            lib.msa_nj_last_stats(ctx.handle, ctypes.byref(st))
+            if s >= 1:
+                kms.append(st.kernel_ms)
+                tms.append(st.total_ms)
+        return nodes, kms, tms, st
+
+    def same_tree(nodes, ref):
+        arr = np.frombuffer(nodes, dtype=np.dtype([("parent", "<u4"), ("c0", "<u4"), ("c1", "<u4"),
+                                                   ("distance", "<f4"), ("level", "<u4")]))
+        return bool((arr["parent"] == ref["parent"]).all() and (arr["c0"] == ref["child0"]).all()
+                    and (arr["c1"] == ref["child1"]).all() and (arr["level"] == ref["level"]).all()
+                    and (arr["distance"].view(np.uint32)
+                         == np.asarray(ref["distance"], np.float32).view(np.uint32)).all())
+
+    nodes, kms, tms, st = run_nj(_lib.MSA_NJ_SYMMETRIC)
+    lin_nodes, lin_kms, _, _ = run_nj(_lib.MSA_NJ_LINEAR)
     kernel_ms = float(np.mean(kms))
     alg = nj_algorithmic_bytes(n)
     out = {"workload": "2000 proteins, 20 clades of 100 (c4 scores, int32 on the device)", "otus": n,
            "joins": n - 1, "kernel_ms": kernel_ms, "total_ms": float(np.mean(tms)), "steps": steps,
            "us_per_join": 1e3 * kernel_ms / (n - 1), "algorithmic_bytes": alg,
            "achieved_GBps": alg / (kernel_ms / 1e3) / 1e9, "cluster_ctas": int(st.cluster),
+           "phase_cycles": {f: int(getattr(st, f)) for f, _ in st._fields_ if f.startswith("cycles")},
+           "linear_order": {"kernel_ms": float(np.mean(lin_kms)),
+                            "us_per_join": 1e3 * float(np.mean(lin_kms)) / (n - 1)},
            "note": "the 16 MB distance matrix stays in L2 (126 MB); the bound is per-join latency"}
     if cpu:
         from oracle import oracle as O
@@ -229,14 +245,13 @@ def nj_leg(lib, ctx, steps: int = 3, cpu: bool = True) -> dict:
             t0 = time.perf_counter()
             ref = O.ref_nj(host.astype(np.float32), n)
             ref_ms = (time.perf_counter() - t0) * 1e3
-            arr = np.frombuffer(nodes, dtype=np.dtype([("parent", "<u4"), ("c0", "<u4"), ("c1", "<u4"),
-                                                       ("distance", "<f4"), ("level", "<u4")]))
             out["cpu_reference"] = {"ms": ref_ms, "cores": 1, "kind": "reference",
                                     "sample": "Museqa njoining::sequential (symmetric), oracle/_ref, full run"}
-            out["tree_matches_reference"] = bool(
-                (arr["parent"] == ref["parent"]).all() and (arr["c0"] == ref["child0"]).all()
-                and (arr["c1"] == ref["child1"]).all()
-                and (arr["distance"].view(np.uint32) == np.asarray(ref["distance"], np.float32).view(np.uint32)).all())
+            out["tree_matches_reference"] = same_tree(nodes, ref)
+            t0 = time.perf_counter()
+            ref_lin = O.ref_nj(host.astype(np.float32), n, "njoining-sequential-linear")
+            out["linear_order"]["cpu_reference_ms"] = (time.perf_counter() - t0) * 1e3
+            out["linear_order"]["tree_matches_reference"] = same_tree(lin_nodes, ref_lin)
     return out
 
 
@@ -272,6 +287,144 @@ def packed_row_fraction(wl, rmax: int = 32) -> float:
     return packed / total if total else 0.0
 
 
+def nw_ceilings(wl, workload: str, nsm: int, sm_mhz: float, lds: float) -> tuple:
+    """Ceilings (GCUPS) of the batched kernel on a workload from rates measured
+    per SM clock: shared-memory profile reads at 2 - f bytes per cell (f: the
+    packed-row share of the cells, from the kernel's plan), the ALU pipe at
+    (1 + f) / 2 lane-ops per cell (64 lanes/clk/SM), and issue at the
+    lane-instructions per cell that ncu counted for this kernel on this
+    workload (profiles/nw_traffic.json), when there is a count. Returns the
+    ceilings, the binding one, f, the counted instructions per cell and the
+    DRAM traffic of one launch."""
+    traffic = inst = None
+    tp = ROOT / "profiles" / "nw_traffic.json"
+    if tp.exists():
+        try:
+            tj = json.loads(tp.read_text())
+            traffic = tj.get(workload)
+            inst = tj.get(workload + "_inst_per_cell")
+        except Exception:
+            traffic = inst = None
+    f = packed_row_fraction(wl)
+    c = {"smem": nsm * (lds / (2.0 - f)) * sm_mhz * 1e6 / 1e9,
+         "alu": nsm * (64.0 / ((1.0 + f) / 2.0)) * sm_mhz * 1e6 / 1e9}
+    if inst:
+        c["issue"] = nsm * (128.0 / inst) * sm_mhz * 1e6 / 1e9
+    bound = min(c, key=c.get)
+    return c, bound, f, inst, traffic
+
+
+class Scorer:
+    """One workload uploaded to the device store of `ctx`, scored into a
+    device triangle with CUDA-event timing on `stream` after an L2 flush."""
+
+    def __init__(self, lib, ctx, stream, wl, device: int):
+        import ctypes
+
+        import torch
+
+        from msa_b200 import ScoringTable, _lib
+        self.lib, self.ctx, self.stream, self.wl = lib, ctx, stream, wl
+        self._lib = _lib
+        self.table = ScoringTable(wl.table)
+        flat, offs, lens = wl.flat_units()
+        n = wl.n
+        u8, u64 = ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint64)
+        self.h = ctypes.c_uint64()
+        _lib.check(lib.msa_seqs_upload(ctx.handle, flat.ctypes.data_as(u8), offs.ctypes.data_as(u64),
+                                       lens.ctypes.data_as(u64), n, ctypes.byref(self.h)), ctx.handle)
+        self.out = torch.empty(n * (n - 1) // 2, dtype=torch.int32, device=f"cuda:{device}")
+        self.flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{device}")   # > 126 MB L2
+
+    def run(self, mode):
+        import ctypes
+        self._lib.check(self.lib.msa_nw_all_pairs(self.ctx.handle, self.h.value, ctypes.byref(self.table._t), mode,
+                                                  ctypes.c_void_p(self.out.data_ptr()), 1), self.ctx.handle)
+
+    def timed(self, mode, steps: int, warmup: int):
+        """Mean step ms (events around the call) and kernel ms (the library's
+        own events around the scoring kernels) over `steps` calls."""
+        import ctypes
+
+        import torch
+        for _ in range(warmup):
+            self.run(mode)
+        torch.cuda.synchronize()
+        ms, kms = [], []
+        for _ in range(steps):
+            self.flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(self.stream)
+            self.run(mode)
+            e1.record(self.stream)
+            e1.synchronize()
+            ms.append(e0.elapsed_time(e1))
+            st = self._lib.MsaNwStats()
+            self.lib.msa_nw_last_stats(self.ctx.handle, ctypes.byref(st))
+            kms.append(st.kernel_ms)
+        return float(np.mean(ms)), float(np.mean(kms)), st
+
+    def release(self):
+        self.lib.msa_seqs_release(self.ctx.handle, self.h.value)
+
+
+def side_workload(lib, ctx, stream, name: str, steps: int, plain_steps: int, sm_mhz: float, lds: float,
+                  device: int) -> dict:
+    """c2 or c4 beside the headline: the persistent kernel and the plain
+    one-launch-per-bucket kernel on the same device store, their bit-identity,
+    and the persistent kernel's roofline fraction at this workload's own
+    packed-row share."""
+    import torch
+
+    from msa_b200 import _lib
+    wl = load_workload(name)
+    sc = Scorer(lib, ctx, stream, wl, device)
+    ms, kms, st = sc.timed(_lib.MSA_NW_PERSISTENT, steps, 3)
+    a = sc.out.clone()
+    pms, pkms, _ = sc.timed(_lib.MSA_NW_PLAIN, plain_steps, 1)
+    agree = bool(torch.equal(a, sc.out))
+    sc.release()
+    cells = wl.cells()
+    nsm = torch.cuda.get_device_properties(device).multi_processor_count
+    c, bound, f, inst, traffic = nw_ceilings(wl, name, nsm, sm_mhz, lds)
+    kg = cells / (kms / 1e3) / 1e9
+    return {"config": workload_config(name, wl), "value": cells / (ms / 1e3) / 1e9, "unit": "GCUPS",
+            "ms_per_step": ms, "steps": steps, "kernel_gcups": kg,
+            "plain": {"value": cells / (pms / 1e3) / 1e9, "ms_per_step": pms, "steps": plain_steps},
+            "speedup_persistent_vs_plain": pms / ms, "bit_identical": agree,
+            "roofline": {"bound": bound, "achieved": kg, "peak": c[bound], "unit": "GCUPS", "frac": kg / c[bound],
+                         "packed_row_fraction": f, "inst_per_cell_counted": inst, "traffic": traffic,
+                         "ceilings_gcups": c}}
+
+
+def ablation(lib, ctx, sc, steps: int) -> dict:
+    """What each part of the batched kernel contributes on the headline
+    workload, beside the plain kernel and the committed kernel (filled in by
+    the caller): the persistent kernel forced to 32-bit lanes; on 16-bit lanes
+    without packed-byte profile rows; and restaging its strip for every column
+    group. Each is a library variant (msa_nw_set_variant) with the same
+    scores, checked against the committed kernel's."""
+    import torch
+
+    from msa_b200 import _lib
+    cells = sc.wl.cells()
+    sc.run(_lib.MSA_NW_PERSISTENT)
+    want = sc.out.clone()
+    out = {}
+    for key, flags, chunk in (("persistent_int32_gcups", _lib.MSA_NW_VARIANT_INT32, 0),
+                              ("persistent_16bit_no_packed_rows_gcups", _lib.MSA_NW_VARIANT_NO_PACKED, 0),
+                              ("persistent_restage_every_group_gcups", 0, 1)):
+        _lib.check(lib.msa_nw_set_variant(ctx.handle, flags, chunk), ctx.handle)
+        try:
+            ms, _, _ = sc.timed(_lib.MSA_NW_PERSISTENT, steps, 1)
+            out[key] = cells / (ms / 1e3) / 1e9
+            out[key.replace("_gcups", "_bit_identical")] = bool(torch.equal(want, sc.out))
+        finally:
+            _lib.check(lib.msa_nw_set_variant(ctx.handle, 0, 0), ctx.handle)
+    out["steps"] = steps
+    return out
+
+
 def probe_rate(ctx, op: int, iters: int = 2048) -> float:
     """Lane-ops (op 15: shared-memory bytes) per SM per clock of one probe form."""
     import ctypes
@@ -297,7 +450,7 @@ def probe_ops(iters: int = 2048) -> dict:
     return res
 
 
-def serve_bench(args):
+def serve_bench(args, emit: bool = True):
     """c5: all-pairs jobs (n U[8,512], lengths U[50,2000], half protein/blosum62,
     half DNA/default) arriving as a Poisson process at `load` x the saturated
     rate; latency = completion - submission per job. The same arrivals are
@@ -331,9 +484,9 @@ def serve_bench(args):
 
     arrivals = arrival_times(5)
 
-    def run_server(window_ms=0.0, arrivals=arrivals):
+    def run_server(window_ms=0.0, arrivals=arrivals, age_ms=0.0):
         stats = [None] * len(jobs)
-        with Server(device=0, batch_window_ms=window_ms) as srv:
+        with Server(device=0, batch_window_ms=window_ms, age_weight_ms=age_ms) as srv:
             ids = [None] * len(jobs)
             start = time.perf_counter()
 
@@ -359,6 +512,17 @@ def serve_bench(args):
                 "p99_over_p50": float(np.percentile(lat, 99) / np.percentile(lat, 50)), "aggregate_gcups": agg,
                 "mean_launches_per_job": float(np.mean([s["launches"] for s in stats]))}
 
+    if args.sweep_age:
+        # Continuous admission with age-weighted shares: weight x arrival-seed sweep.
+        seeds = [int(x) for x in args.arrival_seeds.split(",")]
+        for a in [float(x) for x in args.sweep_age.split(",")]:
+            for seed in seeds:
+                lat, agg, st = run_server(0.0, arrival_times(seed), a)
+                print(json.dumps({"age_weight_ms": a, "arrival_seed": seed, **summary(lat, agg, st),
+                                  "p90_ms": float(np.percentile(lat, 90)), "max_ms": float(lat.max()),
+                                  "saturated_gcups": sat_gcups, "arrival_rate_per_s": rate}), flush=True)
+        return None
+
     if args.sweep_windows:
         # Window x arrival-seed sweep at the same offered load (no plain leg).
         seeds = [int(x) for x in args.arrival_seeds.split(",")]
@@ -378,6 +542,7 @@ def serve_bench(args):
         return None
 
     continuous = summary(*run_server())
+    aged = summary(*run_server(0.0, arrivals, args.age_ms)) if args.age_ms > 0 else None
     windowed = summary(*run_server(args.window_ms)) if args.window_ms > 0 else None
 
     # Same jobs, same arrivals, one at a time through the plain kernel.
@@ -401,10 +566,13 @@ def serve_bench(args):
             "mean_cells_per_job": mean_cells}
     if windowed:
         line["continuous_admission"] = continuous
+    if aged:
+        line["continuous_age_weighted"] = dict(aged, age_weight_ms=args.age_ms)
     line["plain_one_at_a_time"] = {"p50_ms": float(np.percentile(lat_p, 50)), "p99_ms": float(np.percentile(lat_p, 99)),
                                    "aggregate_gcups": agg_p}
     line["data"] = "synthetic (seeded c5 jobs)"
-    print(json.dumps(line))
+    if emit:
+        print(json.dumps(line))
     return line
 
 
@@ -441,12 +609,78 @@ def profile_run(args):
                       "launches": st.launches, "narrow_tasks": st.narrow_tasks}))
 
 
+def shard_line(cfg: dict, world: int, steps: int, warmup: int, step_ms: float, e2e_ms: float, h2d: int, d2h: int,
+               ok, clocks: dict, launches=None, weak=None, roofline=None) -> dict:
+    """The bench line of one job split over `world` ranks (strong scaling:
+    the same job for any number of ranks). `value` is the whole job's GCUPS
+    from the max-over-ranks step time (every part scored, then the exchange
+    into rank 0); `e2e` the same through the public C ABI from pinned host
+    units to the whole matrix in rank 0's host memory."""
+    line = {
+        "metric": METRIC, "value": cfg["cells"] / (step_ms / 1e3) / 1e9, "unit": "GCUPS", "n_gpus": world,
+        "steps": steps, "warmup": warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "strong",
+        "vs_baseline": None, "dtype": "int32/int16x2", "data": "synthetic (seeded)",
+        "config": dict(cfg, parallelism=f"one job split over {world} GPU(s): equal-cell parts of the kernels' task "
+                                        f"list, one NCCL sum-reduce of the disjoint int32 parts into rank 0 "
+                                        f"(the neighbor-joining device)",
+                       l2="flushed (256 MB write) before every timed step"),
+        "matches_single_device": ok,
+        "e2e": {"value": cfg["cells"] / (e2e_ms / 1e3) / 1e9, "unit": "GCUPS", "ms_per_step": e2e_ms,
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "clocks": clocks,
+    }
+    if launches is not None:
+        line["gpu_launches"] = int(launches)
+    if roofline is not None:
+        line["roofline"] = roofline
+    if weak is not None:
+        line["weak_replicas"] = weak
+    return line
+
+
+def timed_steps(step, steps: int, warmup: int, timer, barrier, maxr) -> float:
+    """Mean ms of `steps` calls of step() after `warmup` untimed ones, each
+    timed by timer(step) on this rank; barriers on both sides; the max over
+    ranks of the mean."""
+    for _ in range(warmup):
+        step()
+    barrier()
+    ms = [timer(step) for _ in range(steps)]
+    barrier()
+    return maxr(float(np.mean(ms)))
+
+
+def launch_ranks(nproc: int, script: str, argv: list, timeout_s: int = 3600) -> int:
+    """Runs `script argv` as `nproc` ranks of one node under
+    torch.distributed.run (rendezvous on 127.0.0.1, a free port); returns its
+    exit code. The whole group is killed if it outlives timeout_s."""
+    import signal
+    import socket
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1", f"--nproc-per-node={nproc}",
+           "--master-addr", "127.0.0.1", "--master-port", str(port), str(script), *argv]
+    p = subprocess.Popen(cmd, start_new_session=True)
+    try:
+        return p.wait(timeout=timeout_s)
+    except subprocess.TimeoutExpired:
+        os.killpg(p.pid, signal.SIGTERM)
+        try:
+            p.wait(timeout=60)
+        except subprocess.TimeoutExpired:
+            os.killpg(p.pid, signal.SIGKILL)
+        return 124
+
+
 def shard_bench(args):
-    """One c3 job split over all ranks (one GPU each): every rank scores its
-    part of equal DP cells into a zero-filled device triangle, and one NCCL
-    sum all-reduce assembles the whole matrix on every rank. Strong scaling:
-    the job is the same for any number of ranks. Timed per step from before
-    the part to after the exchange, max over ranks."""
+    """One job split over all ranks (one GPU each): every rank scores its part
+    of equal DP cells into a zero-filled device triangle, and one NCCL
+    sum-reduce assembles the whole matrix on rank 0, the device that runs
+    neighbor-joining. Strong scaling: the job is the same for any number of
+    ranks. Timed per step from before the part to after the exchange, max over
+    ranks. Beside it, `weak_replicas`: every rank scores its own job of the
+    same shape (no data-path collective)."""
     import ctypes
 
     import torch
@@ -468,18 +702,18 @@ def shard_bench(args):
     table = ScoringTable(wl.table)
     flat, offs, lens = wl.flat_units()
     n = wl.n
+    npairs = n * (n - 1) // 2
     u8, u64 = ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint64)
     h = ctypes.c_uint64()
     _lib.check(lib.msa_seqs_upload(ctx.handle, flat.ctypes.data_as(u8), offs.ctypes.data_as(u64),
                                    lens.ctypes.data_as(u64), n, ctypes.byref(h)), ctx.handle)
-    tri = torch.zeros(n * (n - 1) // 2, dtype=torch.int32, device=f"cuda:{local}")
+    tri = torch.zeros(npairs, dtype=torch.int32, device=f"cuda:{local}")
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")
 
     def step():
         tri.zero_()
         shard.score_part(ctx, h.value, table, rank, world, tri.data_ptr())
-        if world > 1:
-            dist.all_reduce(tri, op=dist.ReduceOp.SUM)
+        shard.exchange(tri)
 
     def barrier():
         torch.cuda.synchronize()
@@ -487,27 +721,30 @@ def shard_bench(args):
             dist.barrier()
         torch.cuda.synchronize()
 
-    for _ in range(args.warmup):
-        step()
-    barrier()
-    sampler = ClockSampler(local)
-    sampler.start()
-    ms = []
-    for _ in range(args.steps):
+    def maxr(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def timer(fn):
         flush.zero_()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        step()
+        fn()
         e1.record(stream)
         e1.synchronize()
-        ms.append(e0.elapsed_time(e1))
-    barrier()
+        return e0.elapsed_time(e1)
+
+    sampler = ClockSampler(local)
+    sampler.start()
+    launches0 = ctx.launches
+    step_ms = timed_steps(step, args.steps, args.warmup, timer, barrier, maxr)
+    launches = (ctx.launches - launches0) // max(args.steps + args.warmup, 1)
     clocks = sampler.stop()
-    t = torch.tensor([float(np.mean(ms))], dtype=torch.float64, device=f"cuda:{local}")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    step_ms = float(t.item())
-    # Whole matrix on every rank: check it once against the one-device result.
+
+    # Whole matrix on rank 0: checked against the one-device result.
     ok = None
     if rank == 0:
         full = torch.empty_like(tri)
@@ -515,16 +752,49 @@ def shard_bench(args):
         _lib.check(lib.msa_nw_all_pairs(ctx.handle, h.value, ctypes.byref(table._t), _lib.MSA_NW_PERSISTENT,
                                         ctypes.c_void_p(full.data_ptr()), 1), ctx.handle)
         ok = bool(torch.equal(full, tri))
-        value = cfg["cells"] / (step_ms / 1e3) / 1e9
-        print(json.dumps({
-            "metric": METRIC, "value": value, "unit": "GCUPS", "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": step_ms, "higher_is_better": True, "scaling": "strong",
-            "vs_baseline": None, "dtype": "int32/int16x2", "data": "synthetic (seeded)",
-            "config": dict(cfg, parallelism=f"one job split over {world} GPU(s): equal-cell parts, one NCCL "
-                                            f"sum all-reduce of the int32 triangle",
-                           l2="flushed (256 MB write) before every timed step"),
-            "matches_single_device": ok, "clocks": clocks}))
     lib.msa_seqs_release(ctx.handle, h.value)
+
+    # End to end: pinned host units uploaded on every rank, the part, the
+    # exchange, and the whole matrix read back into rank 0's host memory.
+    pin_units = torch.from_numpy(flat).pin_memory()
+    host_out = torch.empty(npairs, dtype=torch.int32).pin_memory()
+
+    def e2e_step():
+        h2 = ctypes.c_uint64()
+        _lib.check(lib.msa_seqs_upload(ctx.handle, ctypes.cast(pin_units.data_ptr(), u8), offs.ctypes.data_as(u64),
+                                       lens.ctypes.data_as(u64), n, ctypes.byref(h2)), ctx.handle)
+        tri.zero_()
+        shard.score_part(ctx, h2.value, table, rank, world, tri.data_ptr())
+        shard.exchange(tri)
+        if rank == 0:
+            host_out.copy_(tri, non_blocking=True)
+        lib.msa_seqs_release(ctx.handle, h2.value)
+
+    e2e_ms = timed_steps(e2e_step, args.steps, 1, timer, barrier, maxr)
+
+    # Weak replicas: each rank its own job of the same shape, no collective.
+    weak = None
+    if world > 1 and not args.no_extra:
+        own = load_workload(args.workload, rank)
+        sc = Scorer(lib, ctx, stream, own, local)
+        wms = timed_steps(lambda: sc.run(_lib.MSA_NW_PERSISTENT), 1, 1, timer, barrier, maxr)
+        sc.release()
+        weak = {"value": own.cells() * world / (wms / 1e3) / 1e9, "unit": "GCUPS", "ms_per_step": wms,
+                "scaling": "weak", "steps": 1,
+                "parallelism": f"{world} independent replicas, each its own job of this shape (per-rank seed)"}
+
+    if rank == 0:
+        nsm = torch.cuda.get_device_properties(local).multi_processor_count
+        sm_mhz = clocks.get("sm_mhz") or 1965.0
+        lds = probe_rate(ctx, 15)
+        c, bound, f, inst, traffic = nw_ceilings(wl, args.workload, nsm, sm_mhz, lds)
+        per_gpu = cfg["cells"] / (step_ms / 1e3) / 1e9 / world
+        roof = {"bound": bound, "achieved": per_gpu, "peak": c[bound], "unit": "GCUPS", "frac": per_gpu / c[bound],
+                "traffic": traffic, "ceilings_gcups": c, "packed_row_fraction": f,
+                "note": "per GPU: whole-job GCUPS / n_gpus against one GPU's ceilings"}
+        line = shard_line(cfg, world, args.steps, args.warmup, step_ms, e2e_ms,
+                          flat.nbytes + offs.nbytes + lens.nbytes, npairs * 4, ok, clocks, launches, weak, roof)
+        print(json.dumps(line))
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -541,8 +811,13 @@ def main():
     ap.add_argument("--cpu-cells", type=float, default=1.5e10)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-nj", action="store_true", help="skip the neighbor-joining leg")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="skip the c2/c4 legs, the ablation and the serving leg of the default line")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving leg of the default line")
+    ap.add_argument("--side-steps", type=int, default=10, help="timed steps of the c2 and c4 legs")
     ap.add_argument("--shard", action="store_true",
-                    help="one job split over all ranks with an NCCL exchange (strong scaling)")
+                    help="one job split over all ranks with an NCCL exchange (strong scaling; the default "
+                         "when more than one rank runs)")
     ap.add_argument("--profile", choices=["persistent", "plain", "nj"], default=None,
                     help="profiling run: --warmup calls then one call, on the first --n sequences")
     ap.add_argument("--n", type=int, default=0, help="with --profile: use the first N sequences")
@@ -553,16 +828,23 @@ def main():
     ap.add_argument("--sweep-windows", default="",
                     help="with --serve: comma-separated batch windows (ms, 0 = continuous) to sweep instead")
     ap.add_argument("--arrival-seeds", default="5,6,7", help="with --sweep-windows: Poisson arrival seeds")
+    ap.add_argument("--sweep-age", default="",
+                    help="with --serve: comma-separated age weights (ms) of continuous admission to sweep instead")
+    ap.add_argument("--age-ms", type=float, default=10.0,
+                    help="with --serve: age weight (ms) of the age-weighted continuous run (0: skip it)")
     ap.add_argument("--window-ms", type=float, default=60.0,
                     help="with --serve: batch window of the headline serving run (0: continuous admission only)")
     args = ap.parse_args()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        # One process per GPU: start the ranks here when not launched by torchrun.
+        sys.exit(launch_ranks(args.gpus, __file__, sys.argv[1:]))
     if args.probe:
         return probe_ops()
     if args.serve:
         return serve_bench(args)
     if args.impl == "reference":
         return reference_arm(args)
-    if args.shard:
+    if args.shard or _rank_info()[1] > 1:
         return shard_bench(args)
     if args.profile:
         return profile_run(args)
@@ -593,15 +875,8 @@ def main():
     npairs = n * (n - 1) // 2
     u8, u64 = ctypes.POINTER(ctypes.c_uint8), ctypes.POINTER(ctypes.c_uint64)
 
-    h = ctypes.c_uint64()
-    _lib.check(lib.msa_seqs_upload(ctx.handle, flat.ctypes.data_as(u8), offs.ctypes.data_as(u64),
-                                   lens.ctypes.data_as(u64), n, ctypes.byref(h)), ctx.handle)
-    out = torch.empty(npairs, dtype=torch.int32, device=f"cuda:{local}")
-    flush = torch.empty(256 << 20, dtype=torch.uint8, device=f"cuda:{local}")   # > 126 MB L2
-
-    def run(mode):
-        _lib.check(lib.msa_nw_all_pairs(ctx.handle, h.value, ctypes.byref(table._t), mode,
-                                        ctypes.c_void_p(out.data_ptr()), 1), ctx.handle)
+    sc = Scorer(lib, ctx, stream, wl, local)
+    out, flush, run = sc.out, sc.flush, sc.run
 
     def barrier():
         torch.cuda.synchronize()
@@ -660,6 +935,11 @@ def main():
         if s >= 1:
             e2e_ms.append(e0.elapsed_time(e1))
     e2e_ok = bool(torch.equal(host_out, a.cpu()))
+    # Attribution of the persistent kernel's speed-up (rank 0 only, outside
+    # every timed region).
+    abl = None
+    if rank == 0 and not args.no_extra:
+        abl = ablation(lib, ctx, sc, args.plain_steps)
 
     # Max over ranks.
     def maxr(v: float) -> float:
@@ -753,8 +1033,17 @@ def main():
             "clocks": clocks,
             "cpu_baseline": cpu,
         }
+        if abl is not None:
+            line["ablation"] = dict(abl, plain_gcups=plain_gcups, committed_gcups=value)
+        if not args.no_extra:
+            for name in ("c2", "c4"):
+                if name != args.workload:
+                    line[name] = side_workload(lib, ctx, stream, name, args.side_steps, args.plain_steps, sm_mhz, lds,
+                                               local)
         if not args.no_nj:
             line["nj"] = nj_leg(lib, ctx, cpu=not args.no_cpu)
+        if not args.no_extra and not args.no_serve:
+            line["serve"] = serve_bench(args, emit=False)
         print(json.dumps(line))
     if world > 1:
         dist.barrier()

@@ -194,6 +194,18 @@ int msa_nw_part_of_pairs(const uint8_t *units, const uint64_t *offs, const uint6
  * in the reference (its one kernel shape is fixed, hybrid.cu:57). */
 int msa_nw_set_tiles(msa_ctx *ctx, int rows_per_lane, int warps_per_cta);
 
+/* Variants of the persistent kernel, for measuring what each of its parts
+ * contributes (no counterpart in the reference, which has one kernel). Flags:
+ * MSA_NW_VARIANT_INT32 runs every task in 32-bit lanes (one rows sequence at
+ * a time); MSA_NW_VARIANT_NO_PACKED stages every profile row as 16-bit words,
+ * with 32x8 tiles. groups_per_task (0 = the autotuned choice, at most 64) is
+ * how many column groups a task of a rows pair that fits one strip sweeps
+ * after one staging of that strip; 1 restages it for every group. Scores are
+ * the same under every setting. Applies to later calls on the context. */
+#define MSA_NW_VARIANT_INT32 1
+#define MSA_NW_VARIANT_NO_PACKED 2
+int msa_nw_set_variant(msa_ctx *ctx, int flags, uint32_t groups_per_task);
+
 /* Timing breakdown of the context's last msa_nw_all_pairs call (device ms). */
 typedef struct msa_nw_stats {
     double kernel_ms;       /* NW kernels only */
@@ -213,9 +225,11 @@ int msa_nw_last_stats(const msa_ctx *ctx, msa_nw_stats *out);
  * code that must avoid the device synchronisation an allocation can imply.
  * `units` (device) holds the sequences; `offs` and `lens` (host, n entries)
  * locate sequence k at units[offs[k] .. offs[k]+lens[k]); `out` (device) gets
- * n(n-1)/2 int32 scores at i(i-1)/2+j, equal to msa_nw_all_pairs. Runs on
- * `stream` (a cudaStream_t, NULL = legacy default) of the current device and
- * returns after the scores are written.
+ * n(n-1)/2 int32 scores at i(i-1)/2+j, equal to msa_nw_all_pairs (and, like
+ * it, MSA_ERR_UNDEFINED when any sequence holds a GAP unit and the table's
+ * GAP entries lie outside the reference's storage). Runs on `stream` (a
+ * cudaStream_t, NULL = legacy default) of the current device; the call is
+ * blocking: it synchronises `stream` and returns after the scores are written.
  * Scratch is one fixed 16 MiB device array inside this library, shared by all
  * calls on a device and keeping the last call's contents: calls that overlap
  * on the GPU race and must be serialised by the caller. The first call on a
@@ -259,6 +273,26 @@ typedef enum msa_tri_kind {
  */
 int msa_nj(msa_ctx *ctx, const void *tri, int tri_kind, uint32_t n, msa_otu *out_nodes);
 
+/* Removal order of a neighbor-joining run: the reference's two matrix
+ * transforms (src/phylogeny/njoining/impl/sequential.cpp:189-224). After a
+ * join of (x, y), SYMMETRIC swaps y with logical 0 and drops logical 0, so
+ * every index moves down by one; LINEAR swaps y with the last logical OTU and
+ * drops the last. The first-maximum tie-break scans in that order, so the two
+ * give different trees (and always different branch-length bits). */
+typedef enum msa_nj_order_kind {
+    MSA_NJ_SYMMETRIC = 0,
+    MSA_NJ_LINEAR = 1
+} msa_nj_order_kind;
+
+/*
+ * msa_nj with the removal order chosen: MSA_NJ_SYMMETRIC is msa_nj;
+ * MSA_NJ_LINEAR replaces njoining::sequential_linear / hybrid_linear
+ * (src/phylogeny/njoining/impl/sequential.cpp:189-203, 356-358;
+ * src/phylogeny/phylogeny.cpp:30,33,38,40) bit for bit. Other values give
+ * MSA_ERR_INVALID.
+ */
+int msa_nj_order(msa_ctx *ctx, const void *tri, int tri_kind, uint32_t n, int order, msa_otu *out_nodes);
+
 /* Timing of the context's last msa_nj call. The joins run on one cluster of
  * `cluster` CTAs; cycle counts are SM clock cycles by phase, for CTA 0 (scan,
  * wait for the candidates, join, wait until every CTA has read the joined
@@ -292,6 +326,13 @@ typedef struct msa_serve_config {
      * next window's jobs are admitted while the previous one runs and fill
      * its last launches. */
     uint32_t batch_window_us;
+    /* Under continuous admission only: 0 shares each merged launch equally
+     * among the admitted jobs; A > 0 weights job i by 1 + age_i / A (age_i
+     * the time since its submission, in microseconds), so a job that has
+     * waited long, in practice a large one, takes a growing share and the
+     * latency tail shortens while a small job still finishes in a few
+     * launches. */
+    uint32_t age_weight_us;
 } msa_serve_config;
 
 typedef struct msa_job_stats {

@@ -34,11 +34,15 @@ MSA_ERR_TOO_LARGE = 11
 MSA_NW_AUTO = 0
 MSA_NW_PLAIN = 1
 MSA_NW_PERSISTENT = 2
+MSA_NW_VARIANT_INT32 = 1
+MSA_NW_VARIANT_NO_PACKED = 2
 
 MSA_TRI_F32_HOST = 0
 MSA_TRI_F32_DEVICE = 1
 MSA_TRI_I32_HOST = 2
 MSA_TRI_I32_DEVICE = 3
+MSA_NJ_SYMMETRIC = 0
+MSA_NJ_LINEAR = 1
 
 UNIT_END = 0x18
 UNIT_GAP = 0x19
@@ -70,7 +74,8 @@ class MsaNjStats(ctypes.Structure):
 
 class MsaServeConfig(ctypes.Structure):
     _fields_ = [("device", ctypes.c_int), ("hbm_budget_bytes", ctypes.c_uint64), ("max_jobs", ctypes.c_uint32),
-                ("quantum_mcells", ctypes.c_uint32), ("batch_window_us", ctypes.c_uint32)]
+                ("quantum_mcells", ctypes.c_uint32), ("batch_window_us", ctypes.c_uint32),
+                ("age_weight_us", ctypes.c_uint32)]
 
 
 class MsaJobStats(ctypes.Structure):
@@ -120,6 +125,7 @@ _PROTOS = [
                                             ctypes.POINTER(ctypes.c_uint64), ctypes.c_uint32, ctypes.POINTER(MsaTable),
                                             ctypes.c_uint32, ctypes.POINTER(ctypes.c_uint32)]),
     ("msa_nw_set_tiles", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int]),
+    ("msa_nw_set_variant", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32]),
     ("msa_seqs_load_fasta", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(ctypes.c_char_p), ctypes.c_uint32,
                                            ctypes.POINTER(ctypes.c_uint64), ctypes.POINTER(ctypes.c_uint32)]),
     ("msa_seqs_description", ctypes.c_char_p, [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32]),
@@ -134,6 +140,8 @@ _PROTOS = [
     ("msa_nw_last_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(MsaNwStats)]),
     ("msa_nj", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32,
                               ctypes.POINTER(MsaOtu)]),
+    ("msa_nj_order", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_int,
+                                    ctypes.POINTER(MsaOtu)]),
     ("msa_nj_last_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(MsaNjStats)]),
     ("msa_probe_op", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(MsaOpProbe)]),
     ("msa_serve_start", ctypes.c_int, [ctypes.POINTER(MsaServeConfig), ctypes.POINTER(ctypes.c_void_p)]),

@@ -1,12 +1,15 @@
-"""Tile-shape autotuner for the persistent NW kernel.
+"""Autotuner for the persistent NW kernel.
 
     python -m msa_b200.autotune [--write] [--from-json saved_run.log]
 
-Times every (rows per lane, warps per CTA) shape the library is built with on
-seeded workloads of several length classes, prints the table, and with
---write regenerates csrc/autotune.inc (the choice compiled into the library)
-from the fastest shape per class. The measurements behind the committed
-choice are kept next to it in autotune.json.
+For seeded workloads of several length classes it times every (rows per lane,
+warps per CTA) tile shape the library is built with, then, on the fastest
+shape, every number of column groups a single-strip task sweeps after one
+staging of its profile strip (msa_nw_set_variant's groups_per_task: 1 restages
+the strip for every group of W column sequences). It prints the table, and
+with --write regenerates csrc/autotune.inc (the choice compiled into the
+library) from the fastest setting per class. The measurements behind the
+committed choice are kept next to it in autotune.json.
 """
 from __future__ import annotations
 
@@ -20,6 +23,8 @@ import numpy as np
 
 PKG = Path(__file__).resolve().parent
 SHAPES = [(16, 4), (16, 8), (32, 4), (32, 8)]
+CHUNKS = [1, 2, 4, 8, 16]
+DEFAULT_CHUNK = 4
 
 
 def classes():
@@ -39,17 +44,21 @@ def classes():
     ]
 
 
-def time_shape(ctx, wl, shape, reps: int = 3) -> float:
+def time_shape(ctx, wl, shape, reps: int = 3, chunk: int = 0) -> float:
     from . import ScoringTable, _lib, pairwise
     lib = _lib.lib()
     _lib.check(lib.msa_nw_set_tiles(ctx.handle, *shape), ctx.handle)
+    _lib.check(lib.msa_nw_set_variant(ctx.handle, 0, chunk), ctx.handle)
     flat, offs, lens = wl.flat_units()
     best = 0.0
-    for _ in range(reps):
-        pairwise.score_units(flat, offs, lens, ScoringTable(wl.table), _lib.MSA_NW_PERSISTENT)
-        st = pairwise.last_stats()
-        best = max(best, wl.cells() / st.kernel_ms / 1e6)
-    lib.msa_nw_set_tiles(ctx.handle, 0, 0)
+    try:
+        for _ in range(reps):
+            pairwise.score_units(flat, offs, lens, ScoringTable(wl.table), _lib.MSA_NW_PERSISTENT)
+            st = pairwise.last_stats()
+            best = max(best, wl.cells() / st.kernel_ms / 1e6)
+    finally:
+        lib.msa_nw_set_tiles(ctx.handle, 0, 0)
+        lib.msa_nw_set_variant(ctx.handle, 0, 0)
     return best
 
 
@@ -65,7 +74,9 @@ def main():
         table = {}
         for name, wl in classes():
             L = wl.lengths()
-            row = {f"{r}x{w}": round(time_shape(ctx, wl, (r, w)), 1) for r, w in SHAPES}
+            row = {f"{r}x{w}": round(time_shape(ctx, wl, (r, w), chunk=DEFAULT_CHUNK), 1) for r, w in SHAPES}
+            best = max(SHAPES, key=lambda s: row[f"{s[0]}x{s[1]}"])
+            row["groups_per_task"] = {str(g): round(time_shape(ctx, wl, best, chunk=g), 1) for g in CHUNKS}
             row["median_len"] = int(np.median(L))
             table[name] = row
             print(name, row, flush=True)
@@ -86,7 +97,18 @@ def main():
             best = max(SHAPES, key=lambda s: row[f"{s[0]}x{s[1]}"])
             cond = f"med < {bound}" if bound else "true"
             lines.append(f"    if({cond}) return {{{best[0]}, {best[1]}}};   // {row[f'{best[0]}x{best[1]}']} GCUPS")
-        lines += ["    return {32, 8};", "}"]
+        lines += ["    return {32, 8};", "}", "",
+                  "// Column groups per single-strip task, by the same classes.",
+                  "static uint32_t pick_chunk(const SeqStore *st, uint32_t nclean)",
+                  "{",
+                  f"    if(nclean == 0) return {DEFAULT_CHUNK};",
+                  "    const uint32_t med = st->eff[st->clean_sorted[nclean / 2]];"]
+        for name, bound in bounds:
+            gpt = table[name].get("groups_per_task")
+            g = int(max(gpt, key=gpt.get)) if gpt else DEFAULT_CHUNK
+            cond = f"med < {bound}" if bound else "true"
+            lines.append(f"    if({cond}) return {g};" + (f"   // {gpt[str(g)]} GCUPS" if gpt else ""))
+        lines += [f"    return {DEFAULT_CHUNK};", "}"]
         (PKG / "csrc" / "autotune.inc").write_text("\n".join(lines) + "\n")
 
 

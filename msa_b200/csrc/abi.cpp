@@ -315,25 +315,38 @@ static int all_pairs(msa_ctx *ctx, msa_seqs seqs, const msa_table *table, int mo
         for(uint32_t i = 0; i < st->n; ++i) maxlen = std::max<uint64_t>(maxlen, st->plen[i]);
         const int64_t vb = (int64_t) (2 * maxlen + 2048 + 2) * std::max<int64_t>(ext.max_abs, ext.penalty);
         if(vb >= (1ll << 30)) return set_error(ctx, MSA_ERR_TOO_LARGE, "scores could exceed the int32 range");
-        // Tables that are not symmetric make the score depend on orientation:
-        // route every pair through the reference-orientation path.
-        const bool symmetric = table_is_symmetric(ext);
-        std::vector<uint8_t> saved_dirty;
-        std::vector<uint32_t> saved_sorted;
-        if(!symmetric) {
-            saved_dirty = st->dirty;
-            saved_sorted = st->clean_sorted;
-            std::fill(st->dirty.begin(), st->dirty.end(), 1);
-            st->clean_sorted.clear();
-        }
         const uint64_t npairs = (uint64_t) st->n * (st->n ? st->n - 1 : 0) / 2;
+        if(npairs && !out) return MSA_ERR_INVALID;
+        // Tables that are not symmetric make the score depend on orientation:
+        // route every pair through the reference-orientation path for this
+        // call. The store's own plan comes back on every exit, exceptions
+        // included.
+        struct Reorient {
+            SeqStore *st;
+            bool active;
+            std::vector<uint8_t> dirty;
+            std::vector<uint32_t> sorted;
+            Reorient(SeqStore *s, bool on) : st(s), active(on)
+            {
+                if(!active) return;
+                dirty = st->dirty;
+                sorted = st->clean_sorted;
+                std::fill(st->dirty.begin(), st->dirty.end(), 1);
+                st->clean_sorted.clear();
+            }
+            ~Reorient()
+            {
+                if(!active) return;
+                st->dirty.swap(dirty);
+                st->clean_sorted.swap(sorted);
+            }
+        } reorient(st, !table_is_symmetric(ext));
         int32_t *d_out = out;
         if(!out_on_device && npairs) {
             cudaError_t e = ctx->out_tmp.ensure(npairs * sizeof(int32_t));
             if(e) return cuda_error(ctx, e, "output buffer");
             d_out = (int32_t *) ctx->out_tmp.ptr;
         }
-        if(npairs && !out) return MSA_ERR_INVALID;
         rc = nw_run(ctx, st, ext, mode, d_out, part, nparts);
         std::vector<uint32_t> owner;
         if(!out_on_device && npairs && nparts > 1 && !rc) {
@@ -349,10 +362,6 @@ static int all_pairs(msa_ctx *ctx, msa_seqs seqs, const msa_table *table, int mo
                 for(uint32_t a = 2 * k; a < std::min<uint32_t>(2 * k + 2, (uint32_t) cs.size()); ++a)
                     for(uint32_t b = a + 1; b < (uint32_t) cs.size(); ++b) owner[tri(cs[a], cs[b])] = part;
             for(uint64_t q = s.g[part]; q < s.g[part + 1]; ++q) owner[tri(gpairs[2 * q], gpairs[2 * q + 1])] = part;
-        }
-        if(!symmetric) {
-            st->dirty = saved_dirty;
-            st->clean_sorted = saved_sorted;
         }
         if(rc) return rc;
         if(!out_on_device && npairs) {
@@ -394,6 +403,16 @@ int msa_nw_all_pairs_part(msa_ctx *ctx, msa_seqs seqs, const msa_table *table, i
     return msa::all_pairs(ctx, seqs, table, mode, part, nparts, out, out_on_device);
 }
 
+int msa_nw_set_variant(msa_ctx *ctx, int flags, uint32_t groups_per_task)
+{
+    if(!ctx) return MSA_ERR_INVALID;
+    if(flags & ~(MSA_NW_VARIANT_INT32 | MSA_NW_VARIANT_NO_PACKED)) return MSA_ERR_INVALID;
+    if(groups_per_task > 64) return MSA_ERR_INVALID;
+    ctx->nw_variant = flags;
+    ctx->nw_chunk = groups_per_task;
+    return MSA_OK;
+}
+
 int msa_nw_set_tiles(msa_ctx *ctx, int rows_per_lane, int warps_per_cta)
 {
     if(!ctx) return MSA_ERR_INVALID;
@@ -421,13 +440,19 @@ int msa_nj_last_stats(const msa_ctx *ctx, msa_nj_stats *out)
 
 int msa_nj(msa_ctx *ctx, const void *tri, int tri_kind, uint32_t n, msa_otu *out_nodes)
 {
+    return msa_nj_order(ctx, tri, tri_kind, n, MSA_NJ_SYMMETRIC, out_nodes);
+}
+
+int msa_nj_order(msa_ctx *ctx, const void *tri, int tri_kind, uint32_t n, int order, msa_otu *out_nodes)
+{
     if(!ctx) return MSA_ERR_INVALID;
+    if(order != MSA_NJ_SYMMETRIC && order != MSA_NJ_LINEAR) return MSA_ERR_INVALID;
     if(n < 2) return MSA_OK;
     if(!tri || !out_nodes) return MSA_ERR_INVALID;
     if(tri_kind < MSA_TRI_F32_HOST || tri_kind > MSA_TRI_I32_DEVICE) return MSA_ERR_INVALID;
     try {
         cudaSetDevice(ctx->device);
-        return nj_run(ctx, tri, tri_kind, n, out_nodes);
+        return nj_run(ctx, tri, tri_kind, n, order, out_nodes);
     } catch(const std::bad_alloc &) {
         return set_error(ctx, MSA_ERR_NOMEM, "host allocation failed");
     } catch(...) {

@@ -508,8 +508,10 @@ namespace phylogeny {
 namespace {
 
 // The reference's phylogeny names (src/phylogeny/phylogeny.cpp:26-41). All
-// run the device neighbor-joining, which reproduces the sequential
-// symmetric algorithm bit for bit.
+// run the device neighbor-joining; the four that select the linear matrix
+// transform (lines 30, 33, 38, 40) in the linear removal order, which
+// reproduces sequential_linear bit for bit, the others in the symmetric one
+// (sequential_symmetric).
 const std::vector<std::string> &phylogeny_names()
 {
     static const std::vector<std::string> names = {
@@ -520,7 +522,13 @@ const std::vector<std::string> &phylogeny_names()
     return names;
 }
 
-guidetree join(const pairwise::distance_matrix &matrix, size_t count)
+bool linear_name(const std::string &name)
+{
+    return name == "linear" || name == "njoining-linear" || name == "njoining-sequential-linear" ||
+           name == "njoining-distributed-linear";
+}
+
+guidetree join(const pairwise::distance_matrix &matrix, size_t count, int order)
 {
     if(count < 2) return guidetree({}, count);
     if(count != matrix.count()) throw exception("phylogeny count differs from the matrix's");
@@ -529,8 +537,9 @@ guidetree join(const pairwise::distance_matrix &matrix, size_t count)
     const int where = dev ? matrix.device() : device::current();
     msa_ctx *c = context_for(where);
     check_cuda(cudaSetDevice(where), "select device");
-    const int rc = dev ? msa_nj(c, dev, MSA_TRI_I32_DEVICE, (uint32_t) count, nodes.data())
-                       : msa_nj(c, matrix.scores().data(), MSA_TRI_I32_HOST, (uint32_t) count, nodes.data());
+    const int rc = dev ? msa_nj_order(c, dev, MSA_TRI_I32_DEVICE, (uint32_t) count, order, nodes.data())
+                       : msa_nj_order(c, matrix.scores().data(), MSA_TRI_I32_HOST, (uint32_t) count, order,
+                                      nodes.data());
     check_status(rc, c);
     std::vector<otu> out(nodes.size());
     for(size_t k = 0; k < nodes.size(); ++k)
@@ -539,7 +548,9 @@ guidetree join(const pairwise::distance_matrix &matrix, size_t count)
 }
 
 struct b200_njoining : algorithm {
-    guidetree run(const context &ctx) const override { return join(ctx.matrix, ctx.count); }
+    int order;
+    explicit b200_njoining(int o) : order(o) {}
+    guidetree run(const context &ctx) const override { return join(ctx.matrix, ctx.count, order); }
 };
 
 }  // namespace
@@ -553,7 +564,7 @@ bool algorithm::has(const std::string &name)
 std::unique_ptr<algorithm> algorithm::make(const std::string &name)
 {
     if(!has(name)) throw exception(format("unknown phylogeny algorithm '%s'", name.c_str()));
-    return std::unique_ptr<algorithm>(new b200_njoining);
+    return std::unique_ptr<algorithm>(new b200_njoining(linear_name(name) ? MSA_NJ_LINEAR : MSA_NJ_SYMMETRIC));
 }
 
 std::vector<std::string> algorithm::list() { return phylogeny_names(); }
@@ -561,7 +572,7 @@ std::vector<std::string> algorithm::list() { return phylogeny_names(); }
 guidetree run(const pairwise::distance_matrix &matrix, size_t count, const std::string &name)
 {
     if(!algorithm::has(name)) throw exception(format("unknown phylogeny algorithm '%s'", name.c_str()));
-    return join(matrix, count);
+    return join(matrix, count, linear_name(name) ? MSA_NJ_LINEAR : MSA_NJ_SYMMETRIC);
 }
 
 std::string guidetree::newick(const std::vector<std::string> &names) const

@@ -110,6 +110,8 @@ struct msa_ctx {
     // (no device-wide synchronisation on allocation or release).
     cudaMemPool_t pool = nullptr;
     int tile_r = 0, tile_w = 0;   // persistent-kernel tile override (0 = autotuned)
+    int nw_variant = 0;           // msa_nw_set_variant flags (0 = the committed kernel)
+    uint32_t nw_chunk = 0;        // column groups per single-strip task (0 = autotuned)
 };
 
 namespace msa {
@@ -144,7 +146,7 @@ bool table_is_symmetric(const ExtTable &t);
 
 // Bytes of padding before the first sequence in a store's unit buffer.
 constexpr int kUnitFront = 64;
-int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out);
+int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, int order, msa_otu *out);
 
 void release_graphs(msa_ctx *ctx);
 int build_store(msa_ctx *ctx, const uint8_t *units, const uint64_t *offs, const uint64_t *lens, uint32_t n,

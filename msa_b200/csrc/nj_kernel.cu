@@ -1,6 +1,7 @@
 // Neighbor-joining on the device, bit-exact with the reference's
-// njoining::sequential<transform::symmetric>
-// (src/phylogeny/njoining/impl/sequential.cpp:80-346).
+// njoining::sequential<transform::symmetric> and
+// njoining::sequential<transform::linear<2>>
+// (src/phylogeny/njoining/impl/sequential.cpp:80-358).
 //
 // Layout. The reference keeps a packed symmetric matrix and, after every join,
 // swaps the removed OTU y with logical 0 and deletes logical 0
@@ -11,6 +12,13 @@
 // 0 is the increment of t; the swap is one row and one column copy from slot t
 // into slot t + y. Each row of the logical lower triangle is therefore one
 // contiguous run of memory, read with 16-byte loads.
+//
+// The linear order (sequential.cpp:189-203) instead swaps y with the last
+// logical OTU c-1 and drops the last (matrix.cu:443-460 exchanges every
+// off-diagonal pair; the diagonal is zero). No index moves: logical k stays in
+// slot k (t = 0 throughout), and the swap is one row and one column copy from
+// slot c-1 into slot y, or, when x itself was the last, the new node's row and
+// column written into y.
 //
 // Schedule. One thread-block cluster of K CTAs (16 where the device allows,
 // else fewer) runs every join. Hardware cluster barriers (release/acquire)
@@ -98,6 +106,7 @@ struct State {
     uint32_t n, P;
 };
 
+template <bool Linear>
 __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
 {
     cg::cluster_group cluster = cg::this_cluster();
@@ -147,7 +156,8 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
     // 0's data, which the previous join's writes may not have copied yet, so
     // scans read it where it was (slot t - 1): its row there, and column t - 1
     // of every later row.
-    uint32_t pend = kNone, moved = kNone;
+    // `mslot` is the slot where `moved`'s data still is.
+    uint32_t pend = kNone, moved = kNone, mslot = 0;
     bool failed = false;
 
     while(c > 1) {
@@ -177,7 +187,7 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             const uint32_t skip1 = pend == kNone ? kNone : t + pend;
             const uint32_t base4 = t & ~3u;
             const float s_moved = s_moved_sh;
-            auto row_of = [&](uint32_t i) { return D + (size_t) (i == moved ? t - 1 : t + i) * P + base4; };
+            auto row_of = [&](uint32_t i) { return D + (size_t) (i == moved ? mslot : t + i) * P + base4; };
             auto chunk_q = [&](const float4 &d, uint32_t col, uint32_t hi, float si, float &q0, float &q1, float &q2,
                                float &q3) {
                 const float4 s = *reinterpret_cast<const float4 *>(S + col);
@@ -227,7 +237,7 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
                     if(key) lbest = umax64(lbest, ((unsigned long long) key << 32) | (0xffffffffu - ((i << 14) | bg)));
                     // Column `moved` of a later row, from where logical 0's data still is.
                     if(lane == 0 && moved != kNone && i > moved) {
-                        const float dm = __ldcg(D + (size_t) (t + i) * P + t - 1);
+                        const float dm = __ldcg(D + (size_t) (t + i) * P + mslot);
                         const float q = __fsub_rn(__fsub_rn(__fmul_rn(cm2, dm), si), s_moved);
                         offer(pack(order_key(q), i * (i - 1) / 2 + moved), i, moved);
                     }
@@ -249,14 +259,15 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             }
         } else if(pend != kNone) {
             // The new node's row and column, from the distances the last join
-            // computed (ND, indexed by that join's logical order): pairs
-            // (pend, j < pend) and (j > pend, pend) with the reference's
-            // operand order for each.
+            // computed (ND, indexed by that join's logical order: logical j
+            // was j + 1 there in the symmetric order, j in the linear one, and
+            // `moved` was 0 or the last): pairs (pend, j < pend) and
+            // (j > pend, pend) with the reference's operand order for each.
             const uint32_t x = pend;
             const float sx = S[t + x];
             for(uint32_t j = tid; j < c; j += kThreads) {
                 if(j == x) continue;
-                const float d = ND[j == moved ? 0 : j + 1];
+                const float d = ND[j == moved ? (Linear ? mslot : 0u) : (Linear ? j : j + 1)];
                 const float sj = S[t + j];
                 if(j < x) {
                     const float q = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d), sx), sj);
@@ -303,9 +314,15 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             break;
         }
         const uint32_t x = part_xy[wr] >> 16, y = part_xy[wr] & 0xffffu;
+        // The logical index whose data takes y's place (0, or the last in the
+        // linear order), and whether there is such a move: none when y is 0
+        // (symmetric), or when x itself is the last (linear; the new node then
+        // takes y's place).
+        const uint32_t src = Linear ? c - 1 : 0u;
+        const bool mv = Linear ? x != c - 1 : y != 0;
         const float *rx = D + (size_t) (t + x) * P + t;
         const float *ry = D + (size_t) (t + y) * P + t;
-        const float *r0 = D + (size_t) t * P + t;
+        const float *r0 = D + (size_t) (t + src) * P + t;
         // Every load this thread's first join element needs is issued here,
         // before the bookkeeping below: one L2 round trip for all of them.
         const float dxy = __ldcg(rx + y);
@@ -315,7 +332,7 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
         const uint32_t wlo = folder ? 0 : (uint32_t) ((uint64_t) c * rank / F);
         const uint32_t whi = folder ? 0 : (uint32_t) ((uint64_t) c * (rank + 1) / F);
         const uint32_t wi = wlo + tid;
-        const float v0 = (wi < whi && y != 0) ? __ldcg(r0 + wi) : 0.0f;
+        const float v0 = (wi < whi && mv) ? __ldcg(r0 + wi) : 0.0f;
 
         // The scan is over: `moved`'s row sum goes back into its slot.
         if(!folder && tid == 0 && moved != kNone) S[t + moved] = s_moved_sh;
@@ -359,18 +376,21 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             }
         }
         exact = __syncthreads_and(exact);
-        // update_cache (sequential.cpp:210-224): logical 0 takes y's place.
-        // The scanning CTAs keep that row sum aside and put +inf in its slot
-        // and in logical 0's (dropped next) for the next scan.
+        // update_cache (sequential.cpp:189-224): logical `src` takes y's
+        // place. The scanning CTAs keep that row sum aside and put +inf in its
+        // slot, and in logical 0's (symmetric: dropped next), for the next
+        // scan. The linear order's dropped slot c-1 lies past every row the
+        // next scan reads. When the new node takes y's place, its folded sum
+        // arrives there after barrier B.
         if(tid == 0) {
             if(folder) {
-                if(y != 0) S[t + y] = S[t];
+                if(mv) S[t + y] = S[t + src];
             } else {
-                if(y != 0) {
-                    s_moved_sh = S[t];
+                if(mv) {
+                    s_moved_sh = S[t + src];
                     S[t + y] = INFINITY;
                 }
-                S[t] = INFINITY;
+                if(!Linear) S[t] = INFINITY;
             }
         }
         if(timer && rank == 0) mark(2);
@@ -405,7 +425,8 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
                     for(uint32_t i = 0; i < c; ++i) ns = __double2float_rn(__dadd_rn((double) ns, U[i]));
                 }
                 if(lane == 0) cyc[5] += clock64() - f0;
-                if((unsigned) lane < K) cluster.map_shared_rank(S, (unsigned) lane)[t + x] = ns;
+                const uint32_t nslot = Linear && !mv ? y : t + x;
+                if((unsigned) lane < K) cluster.map_shared_rank(S, (unsigned) lane)[nslot] = ns;
             }
             __syncthreads();   // the folded row sum is in this CTA's S
             if(timer) t_last = clock64();
@@ -415,6 +436,36 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             // into y.
             float *wx = D + (size_t) (t + x) * P + t;
             float *wy = D + (size_t) (t + y) * P + t;
+            if(Linear) {
+                // Row/column x get the new distances and row/column c-1 move
+                // into y; or, when x is c-1, the new distances go into y.
+                for(uint32_t i = wi; i < whi; i += kThreads) {
+                    if(mv) {
+                        if(i == c - 1) continue;
+                        if(i == y) {
+                            __stcg(wy + y, __ldcg(r0 + (c - 1)));   // the last one's diagonal
+                            continue;
+                        }
+                        if(i == x) {
+                            __stcg(wx + x, ND[x]);
+                            __stcg(wx + y, ND[c - 1]);
+                            __stcg(wy + x, ND[c - 1]);
+                            continue;
+                        }
+                        const float nd = ND[i];
+                        __stcg(wx + i, nd);
+                        __stcg(D + (size_t) i * P + x, nd);
+                        const float v = i == wi ? v0 : __ldcg(r0 + i);
+                        __stcg(wy + i, v);
+                        __stcg(D + (size_t) i * P + y, v);
+                    } else {
+                        if(i == y || i == x) continue;
+                        const float nd = ND[i];
+                        __stcg(wy + i, nd);
+                        __stcg(D + (size_t) i * P + y, nd);
+                    }
+                }
+            } else
             for(uint32_t i = wi; i < whi; i += kThreads) {
                 if(i == 0 || i == y) {
                     if(i == y && y != 0) __stcg(wy + y, __ldcg(r0));   // logical 0's diagonal
@@ -440,11 +491,21 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             if(timer) mark(4);
         }
 
-        // Logical 0 leaves the window; the new node sits at x - 1 and logical
-        // 0's data at y - 1.
-        pend = x - 1;
-        moved = y != 0 ? y - 1 : kNone;
-        ++t;
+        if(Linear) {
+            // The last logical index leaves; the new node stays at x (or
+            // takes y's place when x was the last) and the last one's data
+            // moves to y.
+            pend = mv ? x : y;
+            moved = mv ? y : kNone;
+            mslot = c - 1;
+        } else {
+            // Logical 0 leaves the window; the new node sits at x - 1 and
+            // logical 0's data at y - 1.
+            pend = x - 1;
+            moved = y != 0 ? y - 1 : kNone;
+            mslot = t;
+            ++t;
+        }
         ++step;
         --c;
     }
@@ -487,6 +548,7 @@ __global__ void row_sums_kernel(const float *__restrict__ D, float *__restrict__
 
 // Largest cluster (16, 8, 4 or 2 CTAs) that can be resident with `smem` bytes
 // of dynamic shared memory per CTA; 0 if none.
+template <bool Linear>
 unsigned pick_cluster(size_t smem)
 {
     for(unsigned k : {16u, 8u, 4u, 2u}) {
@@ -502,7 +564,7 @@ unsigned pick_cluster(size_t smem)
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         int clusters = 0;
-        if(cudaOccupancyMaxActiveClusters(&clusters, nj_cluster_kernel, &cfg) == cudaSuccess && clusters >= 1)
+        if(cudaOccupancyMaxActiveClusters(&clusters, nj_cluster_kernel<Linear>, &cfg) == cudaSuccess && clusters >= 1)
             return k;
         cudaGetLastError();
     }
@@ -511,8 +573,10 @@ unsigned pick_cluster(size_t smem)
 
 }  // namespace njdev
 
-int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out)
+int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, int order, msa_otu *out)
 {
+    const bool linear = order == MSA_NJ_LINEAR;
+    auto kern = linear ? njdev::nj_cluster_kernel<true> : njdev::nj_cluster_kernel<false>;
     cudaStream_t s = ctx->stream;
     const uint32_t P = (n + 3) & ~3u;
     const size_t smem = (size_t) P * 16;   // S, ND (4 B each), U (8 B)
@@ -539,10 +603,9 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out)
     st.n = n;
     st.P = P;
 
-    MSA_CUDA_TRY(ctx, cudaFuncSetAttribute(njdev::nj_cluster_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                           (int) smem));
-    MSA_CUDA_TRY(ctx, cudaFuncSetAttribute(njdev::nj_cluster_kernel, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    const unsigned K = njdev::pick_cluster(smem);
+    MSA_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+    MSA_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    const unsigned K = linear ? njdev::pick_cluster<true>(smem) : njdev::pick_cluster<false>(smem);
     if(K < 2) return set_error(ctx, MSA_ERR_CUDA, "neighbor-joining cluster cannot be resident");
 
     MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[0], s));
@@ -576,7 +639,7 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out)
     cfg.attrs = attr;
     cfg.numAttrs = 1;
     MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[1], s));
-    MSA_CUDA_TRY(ctx, cudaLaunchKernelEx(&cfg, njdev::nj_cluster_kernel, st));
+    MSA_CUDA_TRY(ctx, cudaLaunchKernelEx(&cfg, kern, st));
     MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[2], s));
     ctx->launches++;
     unsigned long long cyc[8] = {0, 0, 0, 0, 0, 0, 0, 0};
@@ -613,8 +676,9 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out)
     if(err == 2) return set_error(ctx, MSA_ERR_UNDEFINED, "no joinable pair: every Q value is NaN");
 
     // star tree (src/phylogeny/njoining/star.cuh:61-72). The kernel records
-    // logical indices; the OTU in each slot follows the same window moves
-    // (slot of x gets the parent; logical 0's OTU moves into y's slot).
+    // logical indices; the OTU in each slot follows the same moves (slot of x
+    // gets the parent; logical 0's OTU, or in the linear order the last one's,
+    // moves into y's slot).
     const uint32_t nodes = 2 * n - 1;
     for(uint32_t k = 0; k < nodes; ++k) {
         out[k].parent = out[k].child[0] = out[k].child[1] = 0xffffffffu;
@@ -625,9 +689,20 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, msa_otu *out)
     for(uint32_t k = 0; k < n; ++k) map[k] = k;
     for(uint32_t k = 0; k + 1 < n; ++k) {
         const uint32_t parent = n + k;
-        const uint32_t a = map[k + rx[k]], b = map[k + ry[k]];
-        map[k + rx[k]] = parent;
-        if(ry[k] != 0) map[k + ry[k]] = map[k];
+        uint32_t a, b;
+        if(linear) {
+            // sequential.cpp:273 then :201-202.
+            const uint32_t c = n - k;
+            a = map[rx[k]];
+            b = map[ry[k]];
+            map[rx[k]] = parent;
+            std::swap(map[ry[k]], map[c - 1]);
+        } else {
+            a = map[k + rx[k]];
+            b = map[k + ry[k]];
+            map[k + rx[k]] = parent;
+            if(ry[k] != 0) map[k + ry[k]] = map[k];
+        }
         const uint32_t c1 = a < b ? a : b, c2 = a < b ? b : a;
         const float d1 = a < b ? rdx[k] : rdy[k], d2 = a < b ? rdy[k] : rdx[k];
         out[c1].distance = d1;

@@ -48,6 +48,7 @@ struct Params {
     int32_t g;
     int32_t *out;
     uint64_t stride;      // boundary-row words per warp
+    int gap_invalid;      // some GAP entry of the table lies outside the reference's storage
     int8_t ext[26 * 26];  // score for units x, y as the reference reads them
     uint8_t valid[26 * 26];
 };
@@ -176,6 +177,16 @@ __global__ void __launch_bounds__(kWPB * 32) noalloc_kernel(Params p, uint32_t *
     const uint64_t gw = (uint64_t) blockIdx.x * kWPB + warp;
     const uint64_t nw = (uint64_t) gridDim.x * kWPB;
     uint32_t *bound = scratch + kHeaderWords + kMetaWords + gw * p.stride;
+    // msa_nw_all_pairs's rule: with such a table, a GAP unit anywhere in any
+    // sequence makes the whole call undefined, wherever the pairs would read it.
+    if(p.gap_invalid) {
+        for(uint64_t q = gw; q < p.n; q += nw) {
+            const uint8_t *u = p.units + offs[q];
+            bool gap = false;
+            for(uint64_t k = lane; k < lens[q]; k += 32) gap |= u[k] == MSA_UNIT_GAP;
+            if(__any_sync(kFull, gap) && lane == 0) atomicOr(err, 1u);
+        }
+    }
     const uint64_t total = (uint64_t) p.n * (p.n - 1) / 2;
     for(uint64_t k = gw; k < total; k += nw) {
         // k = i(i-1)/2 + j, i > j (src/pairwise/pairwise.cpp:73-85).
@@ -267,6 +278,11 @@ extern "C" int msa_nw_all_pairs_noalloc(const uint8_t *units, const uint64_t *of
     p.g = ext.penalty;
     p.out = out;
     p.stride = stride;
+    for(int x = 0; x < 26; ++x)
+        for(int y = 0; y < 26; ++y)
+            if((x == MSA_UNIT_GAP || y == MSA_UNIT_GAP) && x != MSA_UNIT_END && y != MSA_UNIT_END &&
+               !ext.valid[x * 26 + y])
+                p.gap_invalid = 1;
     std::memcpy(p.ext, ext.score, sizeof(p.ext));
     std::memcpy(p.valid, ext.valid, sizeof(p.valid));
 

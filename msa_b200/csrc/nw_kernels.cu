@@ -359,6 +359,7 @@ struct BatchParams {
     const uint64_t *row_task;   // first task of each rows pair (npairs_rows + 1)
     uint64_t ntasks;            // tasks of this launch: task_base .. task_base + ntasks - 1
     uint64_t task_base;
+    uint32_t gchunk;            // column groups per task of a single-strip rows pair
     uint32_t *bound;
     uint64_t bound_stride;
     unsigned long long *counter;
@@ -388,8 +389,8 @@ namespace dev {
 // a long strip's rows) balances the shared-memory data pipe, the bound of
 // 16-bit rows alone, against the ALU pipe and issue: on c3 it measured 16.07
 // TCUPS against 14.81 with no packed rows and 15.96 with R8 = 4 floor(R/8).
-template <int R, bool kNarrow> struct Layout {
-    static constexpr int R8 = kNarrow ? 8 * (R / 16) : 0;
+template <int R, bool kNarrow, bool kPack = true> struct Layout {
+    static constexpr int R8 = kNarrow && kPack ? 8 * (R / 16) : 0;
     static constexpr int R16 = R - R8;
     static constexpr int P16 = R16 / 4;                      // full 16-bit planes
     static constexpr bool kHalf = R16 % 4 != 0;
@@ -413,52 +414,103 @@ __device__ __forceinline__ uint32_t prmt0(uint32_t w)
 // Narrow: word = (s(X1_i, b) + 2g, s(X2_i, b) + 2g) as 16x2 (see Narrow), or
 // bytes (s1_i, s1_i+1, s2_i, s2_i+1) + 2g in the packed planes; rows of X2 past
 // its profile (lp2) score 0. Wide: word = s(X1_i, b) as int32.
-template <int R, bool kNarrow>
+// The profile is read in 16-byte chunks (16 rows of one code), each thread
+// issuing the loads of up to kStageBatch chunks before it converts and stores
+// any, so one staging costs about one L2 round trip instead of one per chunk.
+// Profile rows are 16-byte aligned: the per-sequence pitch is a multiple of
+// 1024 and i0 a multiple of 64; lp2 is a multiple of 1024, so a chunk lies
+// wholly inside or wholly past X2's profile.
+constexpr int kStageBatch = 4;
+
+template <int R, bool kNarrow, bool kPack = true>
 __device__ __forceinline__ void stage_words(uint32_t *sprof, const int8_t *__restrict__ g1, uint32_t lp1,
                                             const int8_t *__restrict__ g2, uint32_t lp2, int i0, int32_t gap = 0)
 {
-    using L = Layout<R, kNarrow>;
+    using L = Layout<R, kNarrow, kPack>;
     constexpr int SH = L::SH;
+    constexpr int CH = 2 * R;                 // 16-byte chunks per code row (32R rows)
+    constexpr int TOTAL = kAlpha * CH;
+    const int nt = blockDim.x;
     if constexpr(kNarrow) {
         static_assert(R % 2 == 0, "16-bit lanes take an even number of rows");
         const uint32_t gg = ((uint32_t) (2 * gap) & 0xffffu) * 0x10001u;
-        constexpr int G2 = 16 * R;       // 2-row groups per code row (32R rows)
-        for(int c = threadIdx.x; c < kAlpha * G2; c += blockDim.x) {
-            const int b = c / G2, q = c - b * G2;
-            const uint32_t va = __ldg(reinterpret_cast<const uint16_t *>(g1 + (size_t) b * lp1 + i0) + q);
-            uint32_t vb = 0;
-            if((uint32_t) (i0 + 2 * q) < lp2) vb = __ldg(reinterpret_cast<const uint16_t *>(g2 + (size_t) b * lp2 + i0) + q);
-            const int row = 2 * q, ln = row / R, r = row - ln * R;
-            uint2 o;
-            o.x = __vadd2(sbyte2<0>(va, vb), gg);
-            o.y = __vadd2(sbyte2<1>(va, vb), gg);
-            uint32_t *code = sprof + b * SH;
-            if(r < 4 * L::P16) {
-                *reinterpret_cast<uint2 *>(code + (r >> 2) * 128 + ln * 4 + (r & 3)) = o;
-            } else if(r < L::R16) {
-                *reinterpret_cast<uint2 *>(code + L::HALF + ln * 2) = o;
-            } else {
-                const int wi = (r - L::R16) >> 1;   // packed word of rows r, r + 1
-                uint32_t pk;
-                asm("prmt.b32 %0, %1, %2, 0x6240;" : "=r"(pk) : "r"(o.x), "r"(o.y));
-                if(wi < 4 * L::P8) code[L::PACK + (wi >> 2) * 128 + ln * 4 + (wi & 3)] = pk;
-                else code[L::PHALF + ln * 2 + (wi - 4 * L::P8)] = pk;
+        for(int c0 = threadIdx.x; c0 < TOTAL; c0 += kStageBatch * nt) {
+            uint4 va[kStageBatch], vb[kStageBatch];
+#pragma unroll
+            for(int u = 0; u < kStageBatch; ++u) {
+                const int c = c0 + u * nt;
+                va[u] = vb[u] = make_uint4(0, 0, 0, 0);
+                if(c < TOTAL) {
+                    const int b = c / CH, m = c - b * CH;
+                    va[u] = __ldg(reinterpret_cast<const uint4 *>(g1 + (size_t) b * lp1 + i0) + m);
+                    if((uint32_t) (i0 + 16 * m) < lp2)
+                        vb[u] = __ldg(reinterpret_cast<const uint4 *>(g2 + (size_t) b * lp2 + i0) + m);
+                }
+            }
+#pragma unroll
+            for(int u = 0; u < kStageBatch; ++u) {
+                const int c = c0 + u * nt;
+                if(c >= TOTAL) break;
+                const int b = c / CH, m = c - b * CH;
+                uint32_t *code = sprof + b * SH;
+                const uint32_t wa[4] = {va[u].x, va[u].y, va[u].z, va[u].w};
+                const uint32_t wb[4] = {vb[u].x, vb[u].y, vb[u].z, vb[u].w};
+#pragma unroll
+                for(int k = 0; k < 8; ++k) {   // two-row group k: rows 16m + 2k, 16m + 2k + 1
+                    uint2 o;
+                    if(k & 1) {
+                        o.x = __vadd2(sbyte2<2>(wa[k >> 1], wb[k >> 1]), gg);
+                        o.y = __vadd2(sbyte2<3>(wa[k >> 1], wb[k >> 1]), gg);
+                    } else {
+                        o.x = __vadd2(sbyte2<0>(wa[k >> 1], wb[k >> 1]), gg);
+                        o.y = __vadd2(sbyte2<1>(wa[k >> 1], wb[k >> 1]), gg);
+                    }
+                    const int row = 16 * m + 2 * k, ln = row / R, r = row - ln * R;
+                    if(r < 4 * L::P16) {
+                        *reinterpret_cast<uint2 *>(code + (r >> 2) * 128 + ln * 4 + (r & 3)) = o;
+                    } else if(r < L::R16) {
+                        *reinterpret_cast<uint2 *>(code + L::HALF + ln * 2) = o;
+                    } else {
+                        const int wi = (r - L::R16) >> 1;   // packed word of rows r, r + 1
+                        uint32_t pk;
+                        asm("prmt.b32 %0, %1, %2, 0x6240;" : "=r"(pk) : "r"(o.x), "r"(o.y));
+                        if(wi < 4 * L::P8) code[L::PACK + (wi >> 2) * 128 + ln * 4 + (wi & 3)] = pk;
+                        else code[L::PHALF + ln * 2 + (wi - 4 * L::P8)] = pk;
+                    }
+                }
             }
         }
     } else {
         static_assert(R % 4 == 0, "32-bit lanes use full planes");
-        constexpr int G = 8 * R;         // 4-row groups per code row
         constexpr int PL = R / 4;        // planes per lane
-        for(int c = threadIdx.x; c < kAlpha * G; c += blockDim.x) {
-            const int b = c / G, rg = c - b * G;
-            const uint32_t va = __ldg(reinterpret_cast<const uint32_t *>(g1 + (size_t) b * lp1 + i0) + rg);
-            const int ln = rg / PL, pl = rg - ln * PL;
-            uint4 o;
-            o.x = (uint32_t) sbyte<0>(va);
-            o.y = (uint32_t) sbyte<1>(va);
-            o.z = (uint32_t) sbyte<2>(va);
-            o.w = (uint32_t) sbyte<3>(va);
-            *reinterpret_cast<uint4 *>(sprof + b * SH + pl * 128 + ln * 4) = o;
+        for(int c0 = threadIdx.x; c0 < TOTAL; c0 += kStageBatch * nt) {
+            uint4 va[kStageBatch];
+#pragma unroll
+            for(int u = 0; u < kStageBatch; ++u) {
+                const int c = c0 + u * nt;
+                va[u] = make_uint4(0, 0, 0, 0);
+                if(c < TOTAL) {
+                    const int b = c / CH, m = c - b * CH;
+                    va[u] = __ldg(reinterpret_cast<const uint4 *>(g1 + (size_t) b * lp1 + i0) + m);
+                }
+            }
+#pragma unroll
+            for(int u = 0; u < kStageBatch; ++u) {
+                const int c = c0 + u * nt;
+                if(c >= TOTAL) break;
+                const int b = c / CH, m = c - b * CH;
+                const uint32_t wa[4] = {va[u].x, va[u].y, va[u].z, va[u].w};
+#pragma unroll
+                for(int k = 0; k < 4; ++k) {   // 4-row group 4m + k
+                    const int rg = 4 * m + k, ln = rg / PL, pl = rg - ln * PL;
+                    uint4 o;
+                    o.x = (uint32_t) sbyte<0>(wa[k]);
+                    o.y = (uint32_t) sbyte<1>(wa[k]);
+                    o.z = (uint32_t) sbyte<2>(wa[k]);
+                    o.w = (uint32_t) sbyte<3>(wa[k]);
+                    *reinterpret_cast<uint4 *>(sprof + b * SH + pl * 128 + ln * 4) = o;
+                }
+            }
         }
     }
 }
@@ -472,14 +524,14 @@ template <bool V> struct Guard { static constexpr bool value = V; };
 // (tend - 1 - lane). Steps run in groups of 8 (the loop bookkeeping of a group
 // is shared by 8 columns); only the fill and drain groups, where some lanes
 // sit outside [0, ncols), test the lane's column.
-template <int R, class K>
+template <int R, class K, bool kPack = true>
 __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, const uint8_t *__restrict__ cols,
                                             int ncols, uint32_t *__restrict__ bound, int i0, int tend,
                                             bool store_bound, int32_t g, int lane, typename K::W (&H)[R])
 {
     using W = typename K::W;
     constexpr bool kB = std::is_same<K, Narrow>::value;
-    using L = Layout<R, kB>;
+    using L = Layout<R, kB, kPack>;
     constexpr int SH = L::SH;
     const W ng = K::splat(-g);
     W diag;
@@ -602,62 +654,107 @@ __device__ __forceinline__ typename K::W pick_row(const typename K::W (&H)[R], i
     return v;
 }
 
-// One task's work for a 16-bit rows pair with strips of 32R rows.
-template <int R>
+// The column sequences of one task: sorted b0, b0 + bstep, ... (ngrp of them
+// for this warp), each against the rows pair (x1, x2) of a job.
+struct TaskCols {
+    const JobView *jv;
+    uint32_t x1, x2, a2;   // rows sequences (original index) and x2's sorted index
+    uint32_t b0, bstep, ngrp;
+};
+
+// One task's work for a 16-bit rows pair with strips of 32R rows. With a
+// single strip (nst == 1) the strip is staged once and swept against every
+// column sequence of the task; otherwise the task has one column sequence per
+// warp and every strip is staged in turn. Only the first staging of a
+// single-strip task and the stagings of a multi-strip task synchronise the
+// CTA, so the loop counts and nst are CTA-uniform.
+template <int R, bool kPack>
 __device__ __noinline__ void narrow_task(uint32_t *sprof, const int8_t *g1, uint32_t lp1, const int8_t *g2,
-                                            uint32_t lp2, int e1, int e2, int nst, bool has, const uint8_t *cols,
-                                            int ncols, uint32_t *bound, int32_t g, int lane, int32_t &r1, int32_t &r2)
+                                         uint32_t lp2, int e1, int e2, int nst, const TaskCols &tc, uint32_t *bound,
+                                         int32_t g, int lane)
 {
     constexpr int SH = 32 * R;
+    const JobView &jv = *tc.jv;
     const int s2 = (e2 - 1) / SH;
-    for(int s = 0; s < nst; ++s) {
-        const int i0 = s * SH;
-        __syncthreads();
-        stage_words<R, true>(sprof, g1, lp1, g2, lp2, i0, g);
-        __syncthreads();
-        if(has) {
-            const bool last = s == nst - 1;
-            const int k1 = last ? (e1 - 1 - i0) / R : 31;
-            Narrow::W H[R];
-            __syncwarp();
-            sweep_strip<R, Narrow>(sprof, cols, ncols, bound, i0, ncols + k1, !last, g, lane, H);
-            __syncwarp();
-            if(s == s2) {
-                const int rr = e2 - 1 - i0;
-                r2 = __shfl_sync(kFull, Narrow::hi(pick_row<R, Narrow>(H, rr % R), g, e2, ncols), rr / R);
+    for(uint32_t t = 0; t < tc.ngrp; ++t) {
+        const uint32_t b = tc.b0 + t * tc.bstep;
+        const bool has = b < jv.nclean;
+        const uint32_t y = has ? jv.sorted[b] : tc.x1;
+        const int ncols = has ? (int) jv.eff[y] : 0;
+        const uint8_t *cols = jv.units + jv.uoff[y];
+        // Row zero of the DP (0 in the T state) as the boundary above the first strip.
+        if(has) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = 0u;
+        int32_t r1 = 0, r2 = 0;
+        for(int s = 0; s < nst; ++s) {
+            const int i0 = s * SH;
+            if(t == 0 || nst > 1) {
+                __syncthreads();
+                stage_words<R, true, kPack>(sprof, g1, lp1, g2, lp2, i0, g);
+                __syncthreads();
             }
-            if(last) {
-                const int rr = e1 - 1 - i0;
-                r1 = __shfl_sync(kFull, Narrow::lo(pick_row<R, Narrow>(H, rr % R), g, e1, ncols), rr / R);
+            if(has) {
+                const bool last = s == nst - 1;
+                const int k1 = last ? (e1 - 1 - i0) / R : 31;
+                Narrow::W H[R];
+                __syncwarp();
+                sweep_strip<R, Narrow, kPack>(sprof, cols, ncols, bound, i0, ncols + k1, !last, g, lane, H);
+                __syncwarp();
+                if(s == s2) {
+                    const int rr = e2 - 1 - i0;
+                    r2 = __shfl_sync(kFull, Narrow::hi(pick_row<R, Narrow>(H, rr % R), g, e2, ncols), rr / R);
+                }
+                if(last) {
+                    const int rr = e1 - 1 - i0;
+                    r1 = __shfl_sync(kFull, Narrow::lo(pick_row<R, Narrow>(H, rr % R), g, e1, ncols), rr / R);
+                }
             }
+        }
+        if(has && lane == 0) {
+            jv.out[tri_index(tc.x1, y)] = r1;
+            if(b != tc.a2) jv.out[tri_index(tc.x2, y)] = r2;
         }
     }
 }
 
-// One rows sequence in 32-bit lanes with strips of 32R rows.
+// One rows sequence (x1 when h == 0, x2 when h == 1) in 32-bit lanes with
+// strips of 32R rows, against the task's column sequences; staging as in
+// narrow_task.
 template <int R>
-__device__ __noinline__ void wide_task(uint32_t *sprof, const int8_t *g1, uint32_t lp1, int e1, int nst,
-                                          bool mine, const uint8_t *cols, int ncols, uint32_t *bound, int32_t g,
-                                          int lane, int32_t &res)
+__device__ __noinline__ void wide_task(uint32_t *sprof, const int8_t *g1, uint32_t lp1, int e1, int nst, int h,
+                                       const TaskCols &tc, uint32_t *bound, int32_t g, int lane)
 {
     constexpr int SH = 32 * R;
-    for(int s = 0; s < nst; ++s) {
-        const int i0 = s * SH;
-        __syncthreads();
-        stage_words<R, false>(sprof, g1, lp1, nullptr, 0, i0);
-        __syncthreads();
-        if(mine) {
-            const bool last = s == nst - 1;
-            const int k1 = last ? (e1 - 1 - i0) / R : 31;
-            Wide::W H[R];
-            __syncwarp();
-            sweep_strip<R, Wide>(sprof, cols, ncols, bound, i0, ncols + k1, !last, g, lane, H);
-            __syncwarp();
-            if(last) {
-                const int rr = e1 - 1 - i0;
-                res = __shfl_sync(kFull, pick_row<R, Wide>(H, rr % R), rr / R);
+    const JobView &jv = *tc.jv;
+    const uint32_t xr = h ? tc.x2 : tc.x1;
+    for(uint32_t t = 0; t < tc.ngrp; ++t) {
+        const uint32_t b = tc.b0 + t * tc.bstep;
+        const bool mine = b < jv.nclean && !(h == 1 && b == tc.a2);
+        const uint32_t y = mine ? jv.sorted[b] : xr;
+        const int ncols = mine ? (int) jv.eff[y] : 0;
+        const uint8_t *cols = jv.units + jv.uoff[y];
+        if(mine) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = (uint32_t) (-(jj + 1) * g);
+        int32_t res = 0;
+        for(int s = 0; s < nst; ++s) {
+            const int i0 = s * SH;
+            if(t == 0 || nst > 1) {
+                __syncthreads();
+                stage_words<R, false>(sprof, g1, lp1, nullptr, 0, i0);
+                __syncthreads();
+            }
+            if(mine) {
+                const bool last = s == nst - 1;
+                const int k1 = last ? (e1 - 1 - i0) / R : 31;
+                Wide::W H[R];
+                __syncwarp();
+                sweep_strip<R, Wide>(sprof, cols, ncols, bound, i0, ncols + k1, !last, g, lane, H);
+                __syncwarp();
+                if(last) {
+                    const int rr = e1 - 1 - i0;
+                    res = __shfl_sync(kFull, pick_row<R, Wide>(H, rr % R), rr / R);
+                }
             }
         }
+        if(mine && lane == 0) jv.out[tri_index(xr, y)] = res;
     }
 }
 
@@ -676,30 +773,33 @@ __device__ __forceinline__ void strip_plan(int rows, int &nst, int &R)
 // Resident CTAs per SM the batched kernel is compiled for (register budget).
 template <int RMAX, int W> struct BatchOcc { static constexpr int value = (RMAX == 32 ? 16 : 24) / W; };
 
-// One task: rows pair k (sorted 2k, 2k+1) of job `jv` against column group
-// `grp` (sorted 2k+1 + grp*W + warp for each warp). All threads of the CTA call it.
-template <int RMAX, int W>
-__device__ __forceinline__ void rows_pair_task(const JobView &jv, uint32_t k, uint32_t grp, uint32_t *sprof_b,
-                                               uint32_t *bound, int warp, int lane)
+// Column groups of W per task for rows pair k of a job with nclean clean
+// sequences: `chunk` groups when its rows fit one strip of 32 RMAX rows (the
+// strip is then staged once for all of them), else one. The host's task
+// tables use the same rule.
+__host__ __device__ __forceinline__ uint32_t groups_per_task(uint32_t e1, int rmax, uint32_t chunk)
+{
+    return e1 <= (uint32_t) (32 * rmax) ? chunk : 1u;
+}
+
+// One task: rows pair k (sorted 2k, 2k+1) of job `jv` against `ngrp` column
+// groups starting at `grp` (group q: sorted 2k+1 + q*W + warp for each warp).
+// All threads of the CTA call it.
+template <int RMAX, int W, bool kPack>
+__device__ __forceinline__ void rows_pair_task(const JobView &jv, uint32_t k, uint32_t grp, uint32_t ngrp,
+                                               uint32_t *sprof_b, uint32_t *bound, int warp, int lane)
 {
     const uint32_t a1 = 2 * k, a2 = min(2 * k + 1, jv.nclean - 1);
-    const uint32_t b = 2 * k + 1 + grp * W + warp;
-    const bool has = b < jv.nclean;
     const uint32_t x1 = jv.sorted[a1], x2 = jv.sorted[a2];
-    const uint32_t y = has ? jv.sorted[b] : x1;
     const int e1 = (int) jv.eff[x1], e2 = (int) jv.eff[x2];
-    const int ncols = has ? (int) jv.eff[y] : 0;
-    const uint8_t *cols = jv.units + jv.uoff[y];
+    dev::TaskCols tc{&jv, x1, x2, a2, 2 * k + 1 + grp * W + warp, (uint32_t) W, ngrp};
 
     if(jv.row_narrow[k]) {
-        // Row zero of the DP (0 in the T state) as the boundary above the first strip.
-        if(has) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = 0u;
         int nst, R;
         dev::strip_plan<RMAX>(e1, nst, R);
-        int32_t r1 = 0, r2 = 0;
         const int8_t *g1 = jv.prof + jv.poff[x1], *g2 = jv.prof + jv.poff[x2];
         const uint32_t lp1 = jv.plp[x1], lp2 = jv.plp[x2];
-#define MSA_NARROW(RR) case RR: dev::narrow_task<RR>(sprof_b, g1, lp1, g2, lp2, e1, e2, nst, has, cols, ncols, bound, jv.g, lane, r1, r2); break;
+#define MSA_NARROW(RR) case RR: dev::narrow_task<RR, kPack>(sprof_b, g1, lp1, g2, lp2, e1, e2, nst, tc, bound, jv.g, lane); break;
         switch(R) {
             MSA_NARROW(2) MSA_NARROW(4) MSA_NARROW(6) MSA_NARROW(8) MSA_NARROW(10) MSA_NARROW(12) MSA_NARROW(14)
             MSA_NARROW(16)
@@ -713,27 +813,20 @@ __device__ __forceinline__ void rows_pair_task(const JobView &jv, uint32_t k, ui
                 break;
         }
 #undef MSA_NARROW
-        if(has && lane == 0) {
-            jv.out[dev::tri_index(x1, y)] = r1;
-            if(b != a2) jv.out[dev::tri_index(x2, y)] = r2;
-        }
     } else {
         for(int h = 0; h < 2; ++h) {
             if(h == 1 && a2 == a1) break;   // CTA-uniform
             const uint32_t xr = h ? x2 : x1;
             const int er = h ? e2 : e1;
-            const bool mine = has && !(h == 1 && b == a2);
-            if(mine) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = (uint32_t) (-(jj + 1) * jv.g);
-            int32_t res = 0;
             const int nst = (er + 32 * RMAX - 1) / (32 * RMAX);
-            dev::wide_task<RMAX>(sprof_b, jv.prof + jv.poff[xr], jv.plp[xr], er, nst, mine, cols, ncols, bound,
-                                 jv.g, lane, res);
-            if(mine && lane == 0) jv.out[dev::tri_index(xr, y)] = res;
+            dev::wide_task<RMAX>(sprof_b, jv.prof + jv.poff[xr], jv.plp[xr], er, nst, h, tc, bound, jv.g, lane);
         }
     }
 }
 
-template <int RMAX, int W>
+// kPack = false stages every profile row as 16-bit words (no packed-byte
+// rows); it exists to measure what the packed rows contribute.
+template <int RMAX, int W, bool kPack = true>
 __global__ void __launch_bounds__(W * 32, BatchOcc<RMAX, W>::value) nw_batched_kernel(BatchParams p)
 {
     extern __shared__ __align__(16) uint32_t sprof_b[];
@@ -752,7 +845,10 @@ __global__ void __launch_bounds__(W * 32, BatchOcc<RMAX, W>::value) nw_batched_k
             const uint32_t mid = (lo + hi + 1) >> 1;
             if(p.row_task[mid] <= q) lo = mid; else hi = mid - 1;
         }
-        rows_pair_task<RMAX, W>(p.job, lo, (uint32_t) (q - p.row_task[lo]), sprof_b, bound, warp, lane);
+        const uint32_t groups = (p.job.nclean - 2 * lo - 1 + W - 1) / W;
+        const uint32_t chunk = groups_per_task(p.job.eff[p.job.sorted[2 * lo]], RMAX, p.gchunk);
+        const uint32_t grp = (uint32_t) (q - p.row_task[lo]) * chunk;
+        rows_pair_task<RMAX, W, kPack>(p.job, lo, grp, min(chunk, groups - grp), sprof_b, bound, warp, lane);
     }
 }
 
@@ -772,7 +868,7 @@ __global__ void __launch_bounds__(W * 32, BatchOcc<RMAX, W>::value) nw_serve_ker
         if(q >= p.ntasks) break;
         const uint4 t = p.tasks[q];
         const JobView jv = p.jobs[t.x];
-        rows_pair_task<RMAX, W>(jv, t.y, t.z, sprof_b, bound, warp, lane);
+        rows_pair_task<RMAX, W, true>(jv, t.y, t.z, 1, sprof_b, bound, warp, lane);
     }
 }
 
@@ -878,7 +974,9 @@ static inline bool narrow_ok(int64_t rows_p, int64_t cols, const ExtTable &t)
     return step * std::min(rows_p, cols) <= 0xffff;
 }
 
-// Batched-kernel tile shapes: rows per lane R and warps per CTA W.
+// Batched-kernel tile shapes (pick_tiles: rows per lane R and warps per CTA
+// W) and column groups per single-strip task (pick_chunk), autotuned; the
+// context may override either (msa_nw_set_tiles, msa_nw_set_variant).
 #include "autotune.inc"
 
 Tiles pick_tiles_for(const SeqStore *st) { return pick_tiles(st, (uint32_t) st->clean_sorted.size()); }
@@ -989,6 +1087,8 @@ struct NwPlan {
     uint32_t launches = 0, narrow_tasks = 0;
     uint64_t cells = 0, pairs = 0;
     uint32_t part = 0, nparts = 1;
+    int variant = 0;            // msa_nw_set_variant flags the plan was built with
+    uint32_t chunk = 0;         // and its groups-per-task override
     cudaGraphExec_t exec = nullptr;
     cudaStream_t captured_on = nullptr;
     ~NwPlan()
@@ -1022,10 +1122,10 @@ void drop_plans_for_store(msa_ctx *ctx, uint64_t serial)
     }
 }
 
-template <int R, int W>
+template <int R, int W, bool kPack = true>
 static int batched_grid(msa_ctx *ctx, uint64_t ntasks, uint64_t *grid)
 {
-    auto kern = nw_batched_kernel<R, W>;
+    auto kern = nw_batched_kernel<R, W, kPack>;
     const size_t smem = (size_t) kAlpha * 32 * R * 4;
     MSA_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
     int bps = 0;
@@ -1035,11 +1135,11 @@ static int batched_grid(msa_ctx *ctx, uint64_t ntasks, uint64_t *grid)
     return MSA_OK;
 }
 
-template <int R, int W>
+template <int R, int W, bool kPack = true>
 static void launch_batched(const NwPlan &pl, cudaStream_t s)
 {
     const size_t smem = (size_t) kAlpha * 32 * R * 4;
-    nw_batched_kernel<R, W><<<(unsigned) pl.batch_grid, W * 32, smem, s>>>(pl.bp);
+    nw_batched_kernel<R, W, kPack><<<(unsigned) pl.batch_grid, W * 32, smem, s>>>(pl.bp);
 }
 
 static int build_plan(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d_out, Tiles tiles,
@@ -1054,6 +1154,8 @@ static int build_plan(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode,
     pl->n = n;
     pl->part = part;
     pl->nparts = nparts;
+    pl->variant = ctx->nw_variant;
+    pl->chunk = ctx->nw_chunk;
 
     const uint32_t nclean = (uint32_t) st->clean_sorted.size();
     const uint64_t nclean_pairs = (uint64_t) nclean * (nclean > 0 ? nclean - 1 : 0) / 2;
@@ -1104,33 +1206,49 @@ static int build_plan(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode,
     uint64_t ntasks = 0;
     uint32_t K = 0;
     uint64_t task_base = 0;
+    uint32_t gchunk = 1;
     if(mode == MSA_NW_PERSISTENT && nclean_pairs > 0) {
         const int SH = 32 * tiles.R;
         K = (nclean + 1) / 2;
-        row_task.assign(K + 1, 0);
         row_narrow.assign(K, 0);
+        std::vector<uint64_t> groups_k(K, 0);
         for(uint32_t k = 0; k < K; ++k) {
-            row_task[k] = ntasks;
             const int64_t ncol = (int64_t) nclean - (2 * (int64_t) k + 1);
             if(ncol <= 0) continue;
             const int64_t rows_p = (int64_t) round_up(st->eff[st->clean_sorted[2 * k]], SH);
             const int64_t cols = st->eff[st->clean_sorted[2 * k + 1]];
-            const bool nar = narrow_ok(rows_p, cols, tbl);
+            const bool nar = narrow_ok(rows_p, cols, tbl) && !(ctx->nw_variant & MSA_NW_VARIANT_INT32);
             row_narrow[k] = nar ? 1 : 0;
-            const uint64_t groups = (uint64_t) (ncol + tiles.W - 1) / tiles.W;
-            if(nar && k >= k_lo && k < k_hi) pl->narrow_tasks += (uint32_t) groups;
-            ntasks += groups;
+            groups_k[k] = (uint64_t) (ncol + tiles.W - 1) / tiles.W;
+            if(nar && k >= k_lo && k < k_hi) pl->narrow_tasks += (uint32_t) groups_k[k];
         }
-        row_task[K] = ntasks;
+        // Tasks of a single-strip rows pair take up to gchunk column groups
+        // (one staging of the strip for all of them) while this part keeps at
+        // least 16 tasks per resident CTA for the work-stealing tail.
+        auto tables = [&](uint32_t chunk) {
+            row_task.assign(K + 1, 0);
+            uint64_t nt = 0;
+            for(uint32_t k = 0; k < K; ++k) {
+                row_task[k] = nt;
+                const uint32_t c = groups_per_task(st->eff[st->clean_sorted[2 * k]], tiles.R, chunk);
+                nt += (groups_k[k] + c - 1) / c;
+            }
+            row_task[K] = nt;
+            return row_task[k_hi] - row_task[k_lo];
+        };
+        int rc;
+        const uint64_t all_groups = tables(1);
+        if(ctx->nw_variant & MSA_NW_VARIANT_NO_PACKED) rc = batched_grid<32, 8, false>(ctx, all_groups, &pl->batch_grid);
+        else if(tiles.R == 16 && tiles.W == 4) rc = batched_grid<16, 4>(ctx, all_groups, &pl->batch_grid);
+        else if(tiles.R == 16 && tiles.W == 8) rc = batched_grid<16, 8>(ctx, all_groups, &pl->batch_grid);
+        else if(tiles.R == 32 && tiles.W == 4) rc = batched_grid<32, 4>(ctx, all_groups, &pl->batch_grid);
+        else rc = batched_grid<32, 8>(ctx, all_groups, &pl->batch_grid);
+        if(rc) return rc;
+        const uint32_t want = ctx->nw_chunk ? ctx->nw_chunk : pick_chunk(st, nclean);
+        for(gchunk = want; gchunk > 1 && tables(gchunk) < 16 * pl->batch_grid; gchunk /= 2) {}
+        ntasks = tables(gchunk);
         // This part's tasks: those of rows pairs [k_lo, k_hi).
         task_base = row_task[k_lo];
-        ntasks = row_task[k_hi] - task_base;
-        int rc;
-        if(tiles.R == 16 && tiles.W == 4) rc = batched_grid<16, 4>(ctx, ntasks, &pl->batch_grid);
-        else if(tiles.R == 16 && tiles.W == 8) rc = batched_grid<16, 8>(ctx, ntasks, &pl->batch_grid);
-        else if(tiles.R == 32 && tiles.W == 4) rc = batched_grid<32, 4>(ctx, ntasks, &pl->batch_grid);
-        else rc = batched_grid<32, 8>(ctx, ntasks, &pl->batch_grid);
-        if(rc) return rc;
         warps_needed = std::max<uint64_t>(warps_needed, pl->batch_grid * tiles.W);
     }
 
@@ -1188,6 +1306,7 @@ static int build_plan(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode,
     bp.row_task = (const uint64_t *) (base + o_rt);
     bp.ntasks = ntasks;
     bp.task_base = task_base;
+    bp.gchunk = gchunk;
     bp.bound = p.bound;
     bp.bound_stride = stride;
     bp.counter = (unsigned long long *) (base + o_cnt);
@@ -1239,7 +1358,8 @@ static cudaError_t enqueue(msa_ctx *ctx, const NwPlan &pl, const SeqStore *st, c
     } else if(pl.bp.ntasks) {
         if((e = cudaMemsetAsync(pl.bp.counter, 0, 64, s))) return e;
         const Tiles t = pl.tiles;
-        if(t.R == 16 && t.W == 4) launch_batched<16, 4>(pl, s);
+        if(pl.variant & MSA_NW_VARIANT_NO_PACKED) launch_batched<32, 8, false>(pl, s);
+        else if(t.R == 16 && t.W == 4) launch_batched<16, 4>(pl, s);
         else if(t.R == 16 && t.W == 8) launch_batched<16, 8>(pl, s);
         else if(t.R == 32 && t.W == 4) launch_batched<32, 4>(pl, s);
         else launch_batched<32, 8>(pl, s);
@@ -1265,6 +1385,7 @@ int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d
 
     const uint32_t nclean = (uint32_t) st->clean_sorted.size();
     const Tiles tiles = mode != MSA_NW_PERSISTENT ? Tiles{0, 0}
+                      : (ctx->nw_variant & MSA_NW_VARIANT_NO_PACKED) ? Tiles{32, 8}
                       : ctx->tile_r ? Tiles{ctx->tile_r, ctx->tile_w} : pick_tiles(st, nclean);
 
     if(!ctx->graphs) ctx->graphs = new GraphCache;
@@ -1273,7 +1394,8 @@ int nw_run(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode, int32_t *d
     for(size_t i = 0; i < plans.size(); ++i) {
         NwPlan *c = plans[i];
         if(c->store_serial == st->serial && c->mode == mode && c->d_out == d_out && c->tiles.R == tiles.R &&
-           c->tiles.W == tiles.W && c->part == part && c->nparts == nparts && same_table(c->tbl, tbl)) {
+           c->tiles.W == tiles.W && c->part == part && c->nparts == nparts && same_table(c->tbl, tbl) &&
+           c->variant == ctx->nw_variant && c->chunk == ctx->nw_chunk) {
             pl = c;
             plans.erase(plans.begin() + i);
             plans.push_back(pl);

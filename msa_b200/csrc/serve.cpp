@@ -23,7 +23,9 @@
 // Two policies share the quantum's cell budget among the admitted jobs:
 //   * continuous (batch_window_us = 0): every job gets an equal share, so a
 //     job's latency is about its own work times the number of jobs sharing the
-//     device;
+//     device; with age_weight_us = A > 0 the shares are weighted by
+//     1 + age / A instead, which moves budget to the jobs that have waited
+//     longest;
 //   * batch windows (batch_window_us = W): a job submitted in window k (from
 //     server start) is admitted at the window's end, the windows are served in
 //     order (older windows take the budget first), and inside a window the
@@ -32,8 +34,10 @@
 //     then close to the window's wait plus the window's work, whatever the
 //     job's own size.
 // Jobs containing sequences that need the reference's orientation (END units
-// inside a sequence, GAP units, a non-symmetric table) are scored at
-// admission by the single-job path on the admission context.
+// inside a sequence, GAP units, a non-symmetric table) are recognised on the
+// host at admission and handed to a third thread with its own context and
+// stream, which scores them one at a time by the single-job path; admission
+// and the merged launches never wait for them.
 #include <algorithm>
 #include <cmath>
 #include <atomic>
@@ -93,12 +97,14 @@ struct Job {
 struct msa_server {
     msa_ctx *ctx = nullptr;   // launch thread
     msa_ctx *adm = nullptr;   // admission thread
+    msa_ctx *ori = nullptr;   // reference-orientation thread
     cudaMemPool_t pool = nullptr;
     cudaStream_t adm_stream = nullptr;   // highest-priority stream of the admission context
-    std::thread worker, admitter;
+    std::thread worker, admitter, orienter;
     std::mutex mu;
-    std::condition_variable cv_work, cv_launch, cv_done;
+    std::condition_variable cv_work, cv_launch, cv_done, cv_oriented;
     std::deque<msa::Job *> pending;
+    std::deque<msa::Job *> oriented;   // admitted jobs for the reference-orientation thread
     std::vector<msa::Job *> admitted;
     std::map<uint64_t, msa::Job *> jobs;
     bool stop = false;
@@ -107,6 +113,7 @@ struct msa_server {
     uint64_t budget = 0, used = 0;
     uint32_t max_jobs = 64, quantum = 0;
     double window_ms = 0;   // admission window (0 = admit at once)
+    double age_ms = 0;      // continuous admission: share weight 1 + age / age_ms (0 = equal shares)
     double t0 = 0;
     // launch resources (worker thread only)
     msa::DevBuf bound, tasks, views, counter, bound2, tasks2, views2, counter2;
@@ -132,62 +139,117 @@ static uint64_t task_cells(const Job *j, uint32_t k, uint32_t g)
     return 2 * e1 * c0 * (bn > b0 ? bn - b0 : 0);
 }
 
-// Admits a job on the admission context: uploads its sequences, table and
-// flags and allocates its output (the score profiles are left to
-// launch_job_profiles, so that the uploads of a batch of jobs do not queue
-// behind one another's kernels). Sets *completed when the job was scored
-// right away (the reference-orientation path); the caller publishes
-// completion under the lock.
-int admit_one(msa_server *srv, Job *j, bool *completed)
+// Whether a job needs the reference's orientation (the single-job path):
+// a sequence with END units before its last letter, an empty one or one with
+// GAP units (the store's "dirty" rule, scan_units), a table that is not
+// symmetric, or fewer than two sequences. Decided on the host from the job's
+// units.
+bool needs_reference_orientation(const Job *j)
 {
-    *completed = false;
+    if(j->n < 2) return true;
+    for(int x = 0; x < 25; ++x)
+        for(int y = 0; y < 25; ++y)
+            if(j->ext.score[x * kAlpha + y] != j->ext.score[y * kAlpha + x]) return true;
+    for(uint32_t i = 0; i < j->n; ++i) {
+        const uint32_t plen = (uint32_t) ((j->lens[i] + 2) / 3 * 3);
+        uint32_t eff = 0;
+        uint8_t dirty = 0, gap = 0;
+        scan_units(j->units.data() + j->offs[i], j->lens[i], plen, &eff, &dirty, &gap);
+        if(dirty) return true;
+    }
+    return false;
+}
+
+uint64_t job_cells(const Job *j)
+{
+    unsigned __int128 s1 = 0, s2 = 0;
+    for(uint32_t i = 0; i < j->n; ++i) { s1 += j->lens[i]; s2 += (unsigned __int128) j->lens[i] * j->lens[i]; }
+    return (uint64_t) ((s1 * s1 - s2) / 2);
+}
+
+// Scores a job in the reference's orientation on the reference-orientation
+// context, synchronously (msa_nw_all_pairs's path: nw_run with every pair of
+// a dirty sequence, or every pair under a non-symmetric table, in the
+// reference's orientation). Device memory comes from the server's pool on
+// that context's stream and is returned there once the scores are on the host.
+int score_oriented(msa_server *srv, Job *j)
+{
+    msa_ctx *ctx = srv->ori;
+    j->cells = job_cells(j);
+    const uint64_t npairs = (uint64_t) j->n * (j->n > 0 ? j->n - 1 : 0) / 2;
+    j->result.assign(npairs, 0);
+    if(j->n < 2) return MSA_OK;
+    SeqStore *st = nullptr;
+    int rc = build_store(ctx, j->units.data(), j->offs.data(), j->lens.data(), j->n, &st);
+    if(rc) return rc;
+    bool symmetric = true;
+    for(int x = 0; x < 25 && symmetric; ++x)
+        for(int y = 0; y < 25; ++y)
+            if(j->ext.score[x * kAlpha + y] != j->ext.score[y * kAlpha + x]) { symmetric = false; break; }
+    if(!symmetric) {
+        std::fill(st->dirty.begin(), st->dirty.end(), 1);
+        st->clean_sorted.clear();
+    }
+    void *out = nullptr;
+    cudaError_t e = cudaMallocFromPoolAsync(&out, npairs * 4, srv->pool, ctx->stream);
+    if(e) {
+        destroy_store_async(st, ctx->stream);
+        return cuda_error(ctx, e, "job output");
+    }
+    rc = nw_run(ctx, st, j->ext, MSA_NW_PERSISTENT, (int32_t *) out);
+    if(!rc) {
+        e = cudaMemcpyAsync(j->result.data(), out, npairs * 4, cudaMemcpyDeviceToHost, ctx->stream);
+        if(!e) e = cudaStreamSynchronize(ctx->stream);
+        if(e) rc = cuda_error(ctx, e, "job scores to host");
+    }
+    drop_plans_for_store(ctx, st->serial);
+    cudaFreeAsync(out, ctx->stream);
+    destroy_store_async(st, ctx->stream);
+    j->launches = 1;
+    return rc;
+}
+
+// Reference-orientation thread: scores the jobs admission handed over, one at
+// a time, and publishes each completion.
+void orientation_loop(msa_server *srv)
+{
+    cudaSetDevice(srv->ori->device);
+    for(;;) {
+        Job *j = nullptr;
+        {
+            std::unique_lock<std::mutex> lk(srv->mu);
+            srv->cv_oriented.wait(lk, [srv] { return srv->stop || !srv->oriented.empty(); });
+            if(srv->stop) return;
+            j = srv->oriented.front();
+            srv->oriented.pop_front();
+        }
+        j->t_admit = now_ms();
+        const int rc = score_oriented(srv, j);
+        std::lock_guard<std::mutex> lk(srv->mu);
+        j->status = rc;
+        j->t_done = now_ms();
+        j->done = true;
+        srv->used -= j->device_bytes;
+        srv->cv_done.notify_all();
+        srv->cv_work.notify_all();
+    }
+}
+
+// Admits a resident job on the admission context: uploads its sequences,
+// table and flags and allocates its output (the score profiles are left to
+// launch_job_profiles, so that the uploads of a batch of jobs do not queue
+// behind one another's kernels). The job holds clean sequences only and a
+// symmetric table (needs_reference_orientation is false).
+int admit_one(msa_server *srv, Job *j)
+{
     msa_ctx *ctx = srv->adm;
     j->t_admit = now_ms();
     int rc = build_store(ctx, j->units.data(), j->offs.data(), j->lens.data(), j->n, &j->st);
     if(rc) return rc;
     SeqStore *st = j->st;
-    unsigned __int128 s1 = 0, s2 = 0;
-    for(uint32_t i = 0; i < j->n; ++i) { s1 += j->lens[i]; s2 += (unsigned __int128) j->lens[i] * j->lens[i]; }
-    j->cells = (uint64_t) ((s1 * s1 - s2) / 2);
+    j->cells = job_cells(j);
     const uint64_t npairs = (uint64_t) j->n * (j->n - 1) / 2;
-    bool symmetric = true;
-    for(int x = 0; x < 25 && symmetric; ++x)
-        for(int y = 0; y < 25; ++y)
-            if(j->ext.score[x * kAlpha + y] != j->ext.score[y * kAlpha + x]) { symmetric = false; break; }
-    bool any_dirty = false;
-    for(uint32_t i = 0; i < j->n; ++i) any_dirty |= st->dirty[i] != 0;
     j->result.assign(npairs, 0);
-    if(any_dirty || !symmetric || j->n < 2) {
-        // Reference-orientation path on the same context, synchronously.
-        if(j->n >= 2) {
-            void *out = nullptr;
-            cudaError_t e = cudaMallocFromPoolAsync(&out, npairs * 4, srv->pool, ctx->stream);
-            if(e) return cuda_error(ctx, e, "job output");
-            std::vector<uint8_t> saved_dirty = st->dirty;
-            std::vector<uint32_t> saved_sorted = st->clean_sorted;
-            if(!symmetric) {
-                std::fill(st->dirty.begin(), st->dirty.end(), 1);
-                st->clean_sorted.clear();
-            }
-            rc = nw_run(ctx, st, j->ext, MSA_NW_PERSISTENT, (int32_t *) out);
-            st->dirty = saved_dirty;
-            st->clean_sorted = saved_sorted;
-            if(!rc) {
-                e = cudaMemcpyAsync(j->result.data(), out, npairs * 4, cudaMemcpyDeviceToHost, ctx->stream);
-                if(!e) e = cudaStreamSynchronize(ctx->stream);
-                if(e) rc = cuda_error(ctx, e, "job scores to host");
-            }
-            drop_plans_for_store(ctx, st->serial);
-            cudaFreeAsync(out, ctx->stream);
-            j->launches = 1;
-        }
-        destroy_store_async(st, ctx->stream);
-        j->st = nullptr;
-        j->t_done = now_ms();
-        j->status = rc;
-        *completed = true;
-        return MSA_OK;   // completed at admission (status carries any error)
-    }
     // Resident job: profiles, 16-bit flags, output triangle.
     plan_rows_pairs(st, j->ext, kServeTiles, j->narrow, j->groups);
     const uint32_t K = (uint32_t) j->narrow.size();
@@ -311,24 +373,38 @@ void admission_loop(msa_server *srv)
                 srv->cv_work.wait_for(lk, std::chrono::microseconds((long long) (wait_ms * 1000)));
             }
         }
-        std::vector<int> status(batch.size(), MSA_OK);
-        std::vector<char> completed(batch.size(), 0);
-        for(size_t i = 0; i < batch.size(); ++i) {
-            bool done = false;
-            status[i] = admit_one(srv, batch[i], &done);
-            completed[i] = done;
+        // Jobs for the single-job path go to the reference-orientation thread
+        // (with their memory reservation) without touching the device here.
+        {
+            std::vector<Job *> resident;
+            bool handed = false;
+            for(Job *j : batch) {
+                if(needs_reference_orientation(j)) {
+                    std::lock_guard<std::mutex> lk(srv->mu);
+                    srv->oriented.push_back(j);
+                    handed = true;
+                } else {
+                    resident.push_back(j);
+                }
+            }
+            if(handed) srv->cv_oriented.notify_one();
+            batch.swap(resident);
+            if(batch.empty()) continue;
         }
+        std::vector<int> status(batch.size(), MSA_OK);
+        for(size_t i = 0; i < batch.size(); ++i) status[i] = admit_one(srv, batch[i]);
         for(size_t i = 0; i < batch.size(); ++i)
-            if(!status[i] && !completed[i]) status[i] = launch_job_profiles(srv, batch[i]);
+            if(!status[i]) status[i] = launch_job_profiles(srv, batch[i]);
         const cudaError_t e = cudaStreamSynchronize(ctx->stream);
         if(e) {
             const int rc = cuda_error(ctx, e, "job admission");
-            for(size_t i = 0; i < batch.size(); ++i) if(!completed[i] && !status[i]) status[i] = rc;
+            for(size_t i = 0; i < batch.size(); ++i) if(!status[i]) status[i] = rc;
         }
         for(size_t i = 0; i < batch.size(); ++i) {
             Job *j = batch[i];
-            if(status[i] || completed[i]) {
-                if(status[i]) { j->status = status[i]; j->t_done = now_ms(); }
+            if(status[i]) {
+                j->status = status[i];
+                j->t_done = now_ms();
                 release_job_device(j, ctx->stream);
             }
         }
@@ -336,7 +412,7 @@ void admission_loop(msa_server *srv)
         bool any = false;
         for(size_t i = 0; i < batch.size(); ++i) {
             Job *j = batch[i];
-            if(status[i] || completed[i]) {
+            if(status[i]) {
                 srv->used -= j->device_bytes;
                 j->done = true;
             } else {
@@ -362,10 +438,10 @@ void worker_loop(msa_server *srv)
     cudaStreamCreateWithFlags(&drain, cudaStreamNonBlocking);
     const cudaStream_t slot_stream[2] = {ctx->own_stream, compute2};
     // Job memory goes back to the pool on this thread's own copy stream, never
-    // on the admission stream: the admission thread may be capturing a CUDA
-    // graph there (jobs scored in the reference's orientation), and a free
-    // enqueued on a capturing stream would become part of that graph. The pool
-    // hands the memory to the next admissions once the free has completed.
+    // on another thread's stream: the reference-orientation thread may be
+    // capturing a CUDA graph on its stream, and a free enqueued on a capturing
+    // stream would become part of that graph. The pool hands the memory to the
+    // next admissions once the free has completed.
     const cudaStream_t release_stream = drain;
     InFlight slots[2];
     for(auto &f : slots) {
@@ -461,6 +537,17 @@ void worker_loop(msa_server *srv)
                 left = rem <= left ? left - rem : 0;
                 a = b;
             }
+        } else if(srv->age_ms > 0) {
+            // Shares weighted by 1 + age / age_ms.
+            const double now = now_ms();
+            std::vector<double> w(active.size());
+            double sum = 0;
+            for(size_t i = 0; i < active.size(); ++i) {
+                w[i] = 1.0 + std::max(0.0, now - active[i]->t_submit) / srv->age_ms;
+                sum += w[i];
+            }
+            for(size_t i = 0; i < active.size(); ++i)
+                quota[i] = std::max<uint64_t>((uint64_t) ((double) budget_cells * w[i] / sum), 1);
         } else {
             std::fill(quota.begin(), quota.end(), std::max<uint64_t>(budget_cells / active.size(), 1));
         }
@@ -595,6 +682,7 @@ int msa_serve_start(const msa_serve_config *cfg, msa_server **out)
         srv = new msa_server;
         int rc = msa_create(cfg->device, &srv->ctx);
         if(!rc) rc = msa_create(cfg->device, &srv->adm);
+        if(!rc) rc = msa_create(cfg->device, &srv->ori);
         if(!rc) {
             cudaMemPoolProps props{};
             props.allocType = cudaMemAllocationTypePinned;
@@ -612,6 +700,7 @@ int msa_serve_start(const msa_serve_config *cfg, msa_server **out)
                 cudaMemPoolSetAttribute(srv->pool, cudaMemPoolAttrReleaseThreshold, &keep);
                 cudaMemPoolSetAttribute(srv->pool, cudaMemPoolReuseAllowInternalDependencies, &no);
                 srv->adm->pool = srv->pool;
+                srv->ori->pool = srv->pool;
                 int least = 0, greatest = 0;
                 cudaDeviceGetStreamPriorityRange(&least, &greatest);
                 if(cudaStreamCreateWithPriority(&srv->adm_stream, cudaStreamNonBlocking, greatest) == cudaSuccess)
@@ -621,6 +710,7 @@ int msa_serve_start(const msa_serve_config *cfg, msa_server **out)
             }
         }
         if(rc) {
+            if(srv->ori) msa_destroy(srv->ori);
             if(srv->adm) msa_destroy(srv->adm);
             if(srv->ctx) msa_destroy(srv->ctx);
             delete srv;
@@ -633,6 +723,7 @@ int msa_serve_start(const msa_serve_config *cfg, msa_server **out)
         srv->max_jobs = cfg->max_jobs ? cfg->max_jobs : 64;
         srv->quantum = cfg->quantum_mcells;
         srv->window_ms = cfg->batch_window_us / 1000.0;
+        srv->age_ms = cfg->age_weight_us / 1000.0;
         rc = warm_server(srv);
         if(rc) {
             srv->bound.release();
@@ -643,6 +734,7 @@ int msa_serve_start(const msa_serve_config *cfg, msa_server **out)
             srv->views2.release();
             srv->counter.release();
             srv->counter2.release();
+            msa_destroy(srv->ori);
             msa_destroy(srv->adm);
             if(srv->adm_stream) cudaStreamDestroy(srv->adm_stream);
             msa_destroy(srv->ctx);
@@ -656,6 +748,7 @@ int msa_serve_start(const msa_serve_config *cfg, msa_server **out)
             srv->cv_done.wait(lk, [srv] { return srv->worker_ready; });
         }
         srv->t0 = now_ms();
+        srv->orienter = std::thread(orientation_loop, srv);
         srv->admitter = std::thread(admission_loop, srv);
         *out = srv;
         return MSA_OK;
@@ -667,8 +760,11 @@ int msa_serve_start(const msa_serve_config *cfg, msa_server **out)
             }
             srv->cv_work.notify_all();
             srv->cv_launch.notify_all();
+            srv->cv_oriented.notify_all();
             if(srv->worker.joinable()) srv->worker.join();
             if(srv->admitter.joinable()) srv->admitter.join();
+            if(srv->orienter.joinable()) srv->orienter.join();
+            if(srv->ori) msa_destroy(srv->ori);
             if(srv->adm) msa_destroy(srv->adm);
             if(srv->adm_stream) cudaStreamDestroy(srv->adm_stream);
             if(srv->ctx) msa_destroy(srv->ctx);
@@ -751,8 +847,10 @@ int msa_serve_stop(msa_server *srv)
         srv->stop = true;
         srv->cv_work.notify_all();
         srv->cv_launch.notify_all();
+        srv->cv_oriented.notify_all();
     }
     if(srv->admitter.joinable()) srv->admitter.join();
+    if(srv->orienter.joinable()) srv->orienter.join();
     if(srv->worker.joinable()) srv->worker.join();
     cudaSetDevice(srv->ctx->device);
     {
@@ -760,6 +858,8 @@ int msa_serve_stop(msa_server *srv)
         std::lock_guard<std::mutex> lk(srv->mu);
         for(Job *j : srv->pending) { j->status = MSA_ERR_QUEUE; j->done = true; }
         srv->pending.clear();
+        for(Job *j : srv->oriented) { j->status = MSA_ERR_QUEUE; j->done = true; }
+        srv->oriented.clear();
         for(Job *j : srv->admitted) { release_job_device(j, srv->adm->stream); j->status = MSA_ERR_QUEUE; j->done = true; }
         srv->admitted.clear();
         srv->cv_done.notify_all();
@@ -767,6 +867,7 @@ int msa_serve_stop(msa_server *srv)
         srv->jobs.clear();
     }
     cudaStreamSynchronize(srv->adm->stream);
+    cudaStreamSynchronize(srv->ori->stream);
     srv->bound.release();
     srv->bound2.release();
     srv->tasks.release();
@@ -775,6 +876,7 @@ int msa_serve_stop(msa_server *srv)
     srv->tasks2.release();
     srv->views2.release();
     srv->counter2.release();
+    msa_destroy(srv->ori);
     msa_destroy(srv->adm);
     if(srv->adm_stream) cudaStreamDestroy(srv->adm_stream);
     msa_destroy(srv->ctx);

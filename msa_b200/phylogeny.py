@@ -9,15 +9,26 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import runtime
-from ._lib import (MSA_TRI_F32_HOST, MSA_TRI_I32_HOST, UNDEFINED_REF, MsaOtu, check, lib)
+from ._lib import (MSA_NJ_LINEAR, MSA_NJ_SYMMETRIC, MSA_TRI_F32_HOST, MSA_TRI_I32_HOST, UNDEFINED_REF, MsaOtu,
+                   check, lib)
 from .pairwise import DistanceMatrix
 
-# src/phylogeny/phylogeny.cpp:26-41. All produce the symmetric-variant tree.
+# src/phylogeny/phylogeny.cpp:26-41. The four names that select the linear
+# matrix transform (hybrid_linear, sequential_linear: lines 30, 33, 38, 40)
+# run the linear removal order; every other name the symmetric one.
 ALGORITHMS = [
     "default", "distributed", "hybrid", "linear", "njoining", "njoining-distributed",
     "njoining-distributed-linear", "njoining-hybrid", "njoining-linear", "njoining-sequential",
     "njoining-sequential-linear", "njoining-symmetric", "sequential", "symmetric",
 ]
+LINEAR = {"linear", "njoining-linear", "njoining-sequential-linear", "njoining-distributed-linear"}
+
+
+def order_of(algorithm: str) -> int:
+    """The removal order a phylogeny algorithm name selects."""
+    if algorithm not in ALGORITHMS:
+        raise RuntimeError(f"unknown phylogeny algorithm '{algorithm}'")
+    return MSA_NJ_LINEAR if algorithm in LINEAR else MSA_NJ_SYMMETRIC
 
 undefined = UNDEFINED_REF
 
@@ -76,8 +87,9 @@ def list() -> "list[str]":  # noqa: A001
     return sorted(ALGORITHMS)
 
 
-def run_triangle(tri: np.ndarray, n: int, device: int | None = None) -> GuideTree:
-    """Neighbor-joining over a packed lower triangle (float32 or int32)."""
+def run_triangle(tri: np.ndarray, n: int, device: int | None = None, order: int = MSA_NJ_SYMMETRIC) -> GuideTree:
+    """Neighbor-joining over a packed lower triangle (float32 or int32), in
+    the symmetric (default) or linear removal order."""
     ctx = runtime.context(device)
     if n < 2:
         return GuideTree([], [], [], [], [], n)
@@ -88,7 +100,7 @@ def run_triangle(tri: np.ndarray, n: int, device: int | None = None) -> GuideTre
         tri = np.ascontiguousarray(tri, np.float32)
         kind = MSA_TRI_F32_HOST
     nodes = (MsaOtu * (2 * n - 1))()
-    check(lib().msa_nj(ctx.handle, tri.ctypes.data_as(ctypes.c_void_p), kind, n, nodes), ctx.handle)
+    check(lib().msa_nj_order(ctx.handle, tri.ctypes.data_as(ctypes.c_void_p), kind, n, order, nodes), ctx.handle)
     arr = np.frombuffer(nodes, dtype=np.dtype([("parent", "<u4"), ("c0", "<u4"), ("c1", "<u4"),
                                                ("distance", "<f4"), ("level", "<u4")]))
     return GuideTree(arr["parent"], arr["c0"], arr["c1"], arr["distance"], arr["level"], n)
@@ -97,10 +109,9 @@ def run_triangle(tri: np.ndarray, n: int, device: int | None = None) -> GuideTre
 def run(matrix: DistanceMatrix, count: int | None = None, algorithm: str = "default",
         device: int | None = None) -> GuideTree:
     """phylogeny::run (src/phylogeny/phylogeny.cuh:245-258)."""
-    if algorithm not in ALGORITHMS:
-        raise RuntimeError(f"unknown phylogeny algorithm '{algorithm}'")
+    order = order_of(algorithm)
     n = matrix.count if count is None else int(count)
     tri = getattr(matrix, "int_scores", None)
     if tri is None:
         tri = matrix.scores
-    return run_triangle(tri, n, device)
+    return run_triangle(tri, n, device, order)

@@ -21,9 +21,12 @@ from .pairwise import ScoringTable
 
 class Server:
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0, max_jobs: int = 0, quantum_mcells: int = 0,
-                 batch_window_ms: float = 0.0):
-        """batch_window_ms > 0 admits jobs at window boundaries (msa_serve_config.batch_window_us)."""
-        cfg = MsaServeConfig(device, hbm_budget_bytes, max_jobs, quantum_mcells, int(round(batch_window_ms * 1000)))
+                 batch_window_ms: float = 0.0, age_weight_ms: float = 0.0):
+        """batch_window_ms > 0 admits jobs at window boundaries (msa_serve_config.batch_window_us);
+        under continuous admission, age_weight_ms > 0 weights each job's share
+        of a launch by 1 + age / age_weight_ms (msa_serve_config.age_weight_us)."""
+        cfg = MsaServeConfig(device, hbm_budget_bytes, max_jobs, quantum_mcells, int(round(batch_window_ms * 1000)),
+                             int(round(age_weight_ms * 1000)))
         h = ctypes.c_void_p()
         check(lib().msa_serve_start(ctypes.byref(cfg), ctypes.byref(h)))
         self.handle = h

@@ -5,8 +5,9 @@ MPI ranks, src/pairwise/needleman/needleman.cpp:31-52).
 Every rank computes the same split (msa_nw_part_of_pairs: runs of the
 kernels' task list with about equal DP cells), scores its own part into a
 zero-filled int32 triangle on its device (msa_nw_all_pairs_part), and one sum
-all-reduce assembles the whole matrix on every rank. The sum is exact: parts
-are disjoint and every other entry is 0.
+reduce assembles the whole matrix on the root rank, the device that runs
+neighbor-joining (a serial chain that runs on one GPU). The sum is exact:
+parts are disjoint and every other entry is 0.
 """
 from __future__ import annotations
 
@@ -17,10 +18,13 @@ import numpy as np
 from ._lib import MSA_NW_PERSISTENT, check, lib
 
 
-def exchange(tri, group=None):
-    """Sums the ranks' partial triangles in place (torch tensor, int32)."""
+def exchange(tri, group=None, root: int = 0):
+    """Sums the ranks' partial triangles into `tri` on rank `root` (torch
+    tensor, int32); other ranks' tensors are left as the reduction leaves
+    them. One rank: nothing to do."""
     import torch.distributed as dist
-    dist.all_reduce(tri, op=dist.ReduceOp.SUM, group=group)
+    if dist.is_initialized() and dist.get_world_size(group) > 1:
+        dist.reduce(tri, dst=root, op=dist.ReduceOp.SUM, group=group)
     return tri
 
 
@@ -33,7 +37,8 @@ def score_part(ctx, seqs: int, table, part: int, nparts: int, out_ptr: int, mode
 
 def all_pairs(flat: np.ndarray, offs: np.ndarray, lens: np.ndarray, table, mode: int = MSA_NW_PERSISTENT,
               group=None, device: int | None = None):
-    """The whole int32 triangle on this rank's device, scored by all ranks."""
+    """The whole int32 triangle on rank 0's device, scored by all ranks (on
+    the other ranks the returned tensor holds no whole matrix)."""
     import torch
     import torch.distributed as dist
 

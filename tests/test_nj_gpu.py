@@ -7,7 +7,7 @@ from pathlib import Path
 import numpy as np
 import pytest
 
-from msa_b200 import phylogeny
+from msa_b200 import _lib, phylogeny
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
@@ -57,6 +57,38 @@ def test_random_matrices_match_oracle(gpu, n, kind):
     assert_same_tree(phylogeny.run_triangle(tri, n), want)
 
 
+LINEAR = _lib.MSA_NJ_LINEAR
+
+
+def test_c1_linear_tree_matches_reference(gpu, golden):
+    """njoining-sequential-linear's tree (the reference's, from the golden
+    fixture) through the linear removal order of the device kernel."""
+    tri = np.array(golden["c1"]["scores"], np.int32)
+    assert_same_tree(phylogeny.run_triangle(tri, 16, order=LINEAR), golden["c1"]["tree_linear"])
+
+
+@pytest.mark.parametrize("n,kind", [(2, "ties"), (3, "ties"), (4, "wide"), (5, "ties"), (6, "wide"), (9, "ties"),
+                                    (17, "ties"), (33, "wide"), (60, "ties"), (120, "ties"), (130, "fraction"),
+                                    (200, "ties"), (300, "tiny"), (700, "wide"), (1100, "ties"), (1500, "wide"),
+                                    (2100, "fraction")])
+def test_random_matrices_linear_order_match_oracle(gpu, n, kind):
+    tri = _matrix(n, kind, np.random.default_rng(1000 + n))
+    want = O.oracle_nj(tri, n, "linear")
+    assert_same_tree(phylogeny.run_triangle(tri, n, order=LINEAR), want)
+
+
+def test_every_name_runs_its_order(gpu, golden):
+    """The four names of the linear transform (src/phylogeny/phylogeny.cpp:30,
+    33, 38, 40) give sequential_linear's tree, the ten others
+    sequential_symmetric's."""
+    from msa_b200 import pairwise
+    tri = np.array(golden["c1"]["scores"], np.int32)
+    dm = pairwise.DistanceMatrix(tri.astype(np.float32), 16)
+    for name in phylogeny.list():
+        want = golden["c1"]["tree_linear"] if name in phylogeny.LINEAR else golden["c1"]["tree"]
+        assert_same_tree(phylogeny.run(dm, 16, algorithm=name), want)
+
+
 def test_all_nan_matrix_is_an_error(gpu):
     from msa_b200._lib import MsaError
     tri = np.full(10 * 9 // 2, np.nan, np.float32)
@@ -91,6 +123,8 @@ def test_c4_tree_matches_reference(gpu):
     tri = pairwise.score_units(flat, offs, lens, ScoringTable("blosum62"))
     assert hashlib.sha256(tri.tobytes()).hexdigest() == g["scores_sha256"]
     assert_same_tree(phylogeny.run_triangle(tri, wl.n), g["tree"])
+    if "tree_linear" in g:
+        assert_same_tree(phylogeny.run_triangle(tri, wl.n, order=LINEAR), g["tree_linear"])
 
 
 def test_small_inputs():

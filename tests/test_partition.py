@@ -1,7 +1,9 @@
 """Splitting one all-pairs job over several devices, host side (no GPU): the
 split covers every pair exactly once, balances DP cells, is deterministic,
-and the one exchange step (a sum all-reduce of zero-filled partial triangles,
-run here over gloo with two ranks) rebuilds the whole matrix exactly."""
+and the one exchange step (a sum-reduce of zero-filled partial triangles into
+rank 0, run here over gloo with two ranks) rebuilds the whole matrix exactly.
+bench.py's rank launcher and its sharded line run here on two gloo ranks,
+with the oracle standing in for the device kernel."""
 import os
 
 import numpy as np
@@ -74,7 +76,8 @@ def _rank_main(rank, world, port, flat, offs, lens, tables, want, nparts, result
         tri = torch.zeros(len(mine), dtype=torch.int32)
         tri[torch.from_numpy(np.nonzero(mine)[0])] = torch.from_numpy(scores[mine].astype(np.int32))
         shard.exchange(tri)
-        result[rank] = bool(np.array_equal(tri.numpy(), want))
+        # The whole matrix lands on rank 0 (the neighbor-joining device).
+        result[rank] = bool(np.array_equal(tri.numpy(), want)) if rank == 0 else True
     finally:
         dist.destroy_process_group()
 
@@ -100,3 +103,19 @@ def test_two_ranks_assemble_the_whole_matrix_over_gloo(golden):
         p.join(120)
         assert p.exitcode == 0
     assert result[0] and result[1]
+
+
+def test_launcher_runs_the_sharded_job_on_two_gloo_ranks(tmp_path):
+    import json
+    from pathlib import Path
+    import bench
+    root = Path(__file__).resolve().parents[1]
+    out = tmp_path / "line.json"
+    rc = bench.launch_ranks(2, str(root / "tests" / "_shard_rank.py"), [str(out)], timeout_s=300)
+    assert rc == 0
+    line = json.loads(out.read_text())
+    assert line["n_gpus"] == 2 and line["scaling"] == "strong" and line["higher_is_better"] is True
+    assert line["matches_single_device"] is True
+    assert line["value"] > 0 and line["unit"] == "GCUPS" and line["ms_per_step"] > 0
+    assert line["e2e"]["h2d_bytes_per_step"] > 0 and line["e2e"]["d2h_bytes_per_step"] == 40 * 39 // 2 * 4
+    assert "sum-reduce" in line["config"]["parallelism"] and line["config"]["pairs"] == 40 * 39 // 2

@@ -85,3 +85,31 @@ def test_noalloc_rejects_requests_beyond_its_limits():
                                              ctypes.c_void_p(out.data_ptr()), None)
     assert rc == _lib.MSA_ERR_TOO_LARGE
     assert b"65536" in _lib.lib().msa_noalloc_last_error()
+
+
+def test_noalloc_gap_unit_in_shorter_sequence_is_undefined_like_the_regular_entry_point():
+    """With a caller's own table every GAP entry lies outside the reference's
+    storage. A GAP unit only in the shorter sequence of a pair must give
+    MSA_ERR_UNDEFINED from both entry points, not scores."""
+    import torch
+    torch.cuda.set_device(0)
+    base = ScoringTable("blosum62").matrix().astype(np.int32)
+    table = ScoringTable.custom(base, 4)
+    wl = W.random_set(74, 6, 60, 120)
+    flat, offs, lens = wl.flat_units(pad3=False)
+    flat = flat.copy()
+    k = int(np.argmin(lens))
+    flat[int(offs[k]) + int(lens[k]) // 2] = _lib.UNIT_GAP
+    with pytest.raises(_lib.MsaError) as regular:
+        pairwise.score_units(flat, offs, lens, table, _lib.MSA_NW_PERSISTENT)
+    assert regular.value.status == _lib.MSA_ERR_UNDEFINED
+    d_units = torch.from_numpy(flat).to("cuda:0")
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        with pytest.raises(_lib.MsaError) as na:
+            _noalloc(d_units, offs, lens, wl.n, table, stream)
+        assert na.value.status == _lib.MSA_ERR_UNDEFINED
+    # Without the GAP unit the same call scores as before.
+    flat2, _, _ = wl.flat_units(pad3=False)
+    got = _noalloc(torch.from_numpy(flat2.copy()).to("cuda:0"), offs, lens, wl.n, table, stream)
+    assert np.array_equal(got, pairwise.score_units(flat2, offs, lens, table, _lib.MSA_NW_PERSISTENT))
