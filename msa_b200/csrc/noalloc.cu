@@ -50,7 +50,6 @@ struct Params {
     uint64_t stride;      // boundary-row words per warp
     int gap_invalid;      // some GAP entry of the table lies outside the reference's storage
     int8_t ext[26 * 26];  // score for units x, y as the reference reads them
-    uint8_t valid[26 * 26];
 };
 
 template <int K>
@@ -70,8 +69,7 @@ __device__ __forceinline__ uint32_t unit_at(const uint8_t *s, uint64_t len, int6
 // the first END unit, END columns copy their left neighbour, the padded column
 // width is swept (src/pairwise/needleman/impl/sequential.cpp:29-68).
 __device__ void score_pair(const Params &p, const uint8_t *rows, uint64_t lr, const uint8_t *cols, uint64_t lc,
-                           int8_t *sprof, const int8_t *stab, uint32_t *bound, int lane, int32_t &result,
-                           uint32_t *err)
+                           int8_t *sprof, const int8_t *stab, uint32_t *bound, int lane, int32_t &result)
 {
     const int plen_r = (int) ((lr + 2) / 3 * 3), ncols = (int) ((lc + 2) / 3 * 3);
     // Effective rows: up to the first END unit.
@@ -107,8 +105,10 @@ __device__ void score_pair(const Params &p, const uint8_t *rows, uint64_t lr, co
 #pragma unroll
                 for(int k = 0; k < 4; ++k) {
                     const uint32_t x = xr[4 * q + k];
+                    // Entries outside the reference's storage all involve
+                    // the GAP unit; the kernel's GAP rule has already flagged
+                    // any call that could read one (they stage as 0).
                     const int idx = (int) x * 26 + b;
-                    if(b != MSA_UNIT_END && !p.valid[idx] && i0 + lane * kR + 4 * q + k < nrows) atomicOr(err, 1u);
                     w[q] |= ((uint32_t) (uint8_t) stab[idx]) << (8 * k);
                 }
             }
@@ -198,7 +198,7 @@ __global__ void __launch_bounds__(kWPB * 32) noalloc_kernel(Params p, uint32_t *
         const uint64_t r = bi > bj ? i : j, c = bi > bj ? j : i;   // sequential.cpp:87-91
         int32_t res = 0;
         score_pair(p, p.units + offs[r], lens[r], p.units + offs[c], lens[c], sprof_all + warp * 26 * kSH, stab, bound,
-                   lane, res, err);
+                   lane, res);
         if(lane == 0) p.out[k] = res;
     }
 }
@@ -284,7 +284,6 @@ extern "C" int msa_nw_all_pairs_noalloc(const uint8_t *units, const uint64_t *of
                !ext.valid[x * 26 + y])
                 p.gap_invalid = 1;
     std::memcpy(p.ext, ext.score, sizeof(p.ext));
-    std::memcpy(p.valid, ext.valid, sizeof(p.valid));
 
     int sms = 0, bps = 0;
     if(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
