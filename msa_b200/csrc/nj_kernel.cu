@@ -323,57 +323,65 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
         const float *rx = D + (size_t) (t + x) * P + t;
         const float *ry = D + (size_t) (t + y) * P + t;
         const float *r0 = D + (size_t) (t + src) * P + t;
-        // Every load this thread's first join element needs is issued here,
-        // before the bookkeeping below: one L2 round trip for all of them.
+        // Every load this thread's first two join elements need is issued
+        // here, before the bookkeeping below: one L2 round trip for all of
+        // them (c <= 2048); later elements are loaded two iterations ahead.
         const float dxy = __ldcg(rx + y);
-        float a = (uint32_t) tid < c ? __ldcg(rx + tid) : 0.0f, b = (uint32_t) tid < c ? __ldcg(ry + tid) : 0.0f;
+        float a0 = (uint32_t) tid < c ? __ldcg(rx + tid) : 0.0f, b0 = (uint32_t) tid < c ? __ldcg(ry + tid) : 0.0f;
+        const uint32_t i1 = tid + kThreads;
+        float a1 = i1 < c ? __ldcg(rx + i1) : 0.0f, b1 = i1 < c ? __ldcg(ry + i1) : 0.0f;
         // This thread's first element of the write slice (CTAs 0..F-1):
-        // logical 0's entry, loaded now so the writes wait for no load.
+        // the moved row's entry, loaded now so the writes wait for no load.
         const uint32_t wlo = folder ? 0 : (uint32_t) ((uint64_t) c * rank / F);
         const uint32_t whi = folder ? 0 : (uint32_t) ((uint64_t) c * (rank + 1) / F);
         const uint32_t wi = wlo + tid;
         const float v0 = (wi < whi && mv) ? __ldcg(r0 + wi) : 0.0f;
 
-        // The scan is over: `moved`'s row sum goes back into its slot.
-        if(!folder && tid == 0 && moved != kNone) S[t + moved] = s_moved_sh;
-
-        // raise_candidate (sequential.cpp:142-152) and the join record.
-        if(rank == 0 && tid == 0) {
-            const float pairsum = __fsub_rn(S[t + x], S[t + y]);
-            const float den = (float) (2u * (c - 2));
-            const float q = __fdiv_rn(pairsum, den);
-            float dx = __double2float_rn(__dadd_rn(__dmul_rn(0.5, (double) dxy), (double) q));
-            float dy = __fsub_rn(dxy, dx);
-            // The last join divides by 2(c-2) = 0; for 0/0 the reference's x86
-            // SSE arithmetic yields the default NaN 0xFFC00000 and propagates it
-            // into dx and dy, where the GPU would give its canonical 0x7FFFFFFF.
-            if(dx != dx) dx = __uint_as_float(0xFFC00000u);
-            if(dy != dy) dy = __uint_as_float(0xFFC00000u);
-            st.rec_x[step] = x;
-            st.rec_y[step] = y;
-            st.rec_dx[step] = dx;
-            st.rec_dy[step] = dy;
-        }
-        __syncthreads();   // S[x], S[y] are read before the row sums change
+        // The scanning CTAs hold +inf in `moved`'s slot of S during a scan;
+        // its row sum is s_moved_sh, which the join reads in its place.
+        const uint32_t mvd = folder ? kNone : moved;
+        const float s_moved = s_moved_sh;
 
         // join_pair (sequential.cpp:247-267). D[i][x] and D[i][y] are read as
         // row x and row y (the matrix is symmetric bit for bit); i = x and
-        // i = y read the diagonal and D[x][y], as the reference does.
+        // i = y read the diagonal and D[x][y], as the reference does. The
+        // thread of element y in CTA 0 also computes raise_candidate
+        // (sequential.cpp:142-152) from the row sums before this join's
+        // update (S[x] is not updated here, S[y] is read before it is).
         bool exact = true;
-        {
-            for(uint32_t i = tid; i < c; i += kThreads) {
-                const uint32_t in = i + kThreads;
-                const float an = in < c ? __ldcg(rx + in) : 0.0f, bn = in < c ? __ldcg(ry + in) : 0.0f;
-                const float prev = __fadd_rn(a, b);
-                const double u = __dmul_rn((double) __fsub_rn(prev, dxy), 0.5);
-                const float nd = __double2float_rn(u);
-                U[i] = u;
-                ND[i] = nd;
-                exact = exact && ((double) nd == u);
-                if(i != x) S[t + i] = __double2float_rn(__dadd_rn((double) S[t + i], __dsub_rn(u, (double) prev)));
-                a = an;
-                b = bn;
+        for(uint32_t i = tid; i < c; i += kThreads) {
+            const uint32_t in = i + 2 * kThreads;
+            const float an = in < c ? __ldcg(rx + in) : 0.0f, bn = in < c ? __ldcg(ry + in) : 0.0f;
+            const float prev = __fadd_rn(a0, b0);
+            const double u = __dmul_rn((double) __fsub_rn(prev, dxy), 0.5);
+            const float nd = __double2float_rn(u);
+            U[i] = u;
+            ND[i] = nd;
+            exact = exact && ((double) nd == u);
+            const float s_old = i == mvd ? s_moved : S[t + i];
+            if(rank == 0 && i == y) {
+                const float sx = x == mvd ? s_moved : S[t + x];
+                const float pairsum = __fsub_rn(sx, s_old);
+                const float den = (float) (2u * (c - 2));
+                const float q = __fdiv_rn(pairsum, den);
+                float dx = __double2float_rn(__dadd_rn(__dmul_rn(0.5, (double) dxy), (double) q));
+                float dy = __fsub_rn(dxy, dx);
+                // The last join divides by 2(c-2) = 0; for 0/0 the reference's
+                // x86 SSE arithmetic yields the default NaN 0xFFC00000 and
+                // propagates it into dx and dy, where the GPU would give its
+                // canonical 0x7FFFFFFF.
+                if(dx != dx) dx = __uint_as_float(0xFFC00000u);
+                if(dy != dy) dy = __uint_as_float(0xFFC00000u);
+                st.rec_x[step] = x;
+                st.rec_y[step] = y;
+                st.rec_dx[step] = dx;
+                st.rec_dy[step] = dy;
             }
+            if(i != x) S[t + i] = __double2float_rn(__dadd_rn((double) s_old, __dsub_rn(u, (double) prev)));
+            a0 = a1;
+            b0 = b1;
+            a1 = an;
+            b1 = bn;
         }
         exact = __syncthreads_and(exact);
         // update_cache (sequential.cpp:189-224): logical `src` takes y's
@@ -394,43 +402,43 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             }
         }
         if(timer && rank == 0) mark(2);
-        cluster_arrive();   // B: every read of rows x, y and 0 is done
-        cluster_wait();
+        cluster_arrive();   // B: every read of rows x, y and the moved row is done
 
         if(folder) {
             // Serial fold of the new row sum, i ascending. When every update is
             // a float value, the double add rounded to float equals a float add
             // (double has >= 2*24+2 significand bits), so the short float chain
-            // is used; otherwise the literal double one. Warp 0 runs it.
+            // is used; otherwise the literal double one. Warp 0 runs it (every
+            // lane the same chain, reading ND by broadcast 16-byte loads that
+            // do not depend on the chain) while barrier B completes: the fold
+            // reads only this CTA's ND and U, written before this thread's
+            // __syncthreads_and above. Its result goes into every CTA's S only
+            // after B, when no CTA still updates its row sums for this join.
+            float ns = 0.0f;
             if(warp == 0) {
                 const unsigned long long f0 = clock64();
-                float ns = 0.0f;
                 if(exact) {
-                    // Each chunk of 32 updates is loaded one per lane (the next
-                    // chunk while this one is added) and handed out by
-                    // shuffles; every lane adds the same chain.
-                    float v = (uint32_t) lane < c ? ND[lane] : 0.0f;
-                    for(uint32_t base = 0; base < c; base += 32) {
-                        const float cur = v;
-                        const uint32_t nxt = base + 32 + lane;
-                        v = nxt < c ? ND[nxt] : 0.0f;
-                        const uint32_t m = min(32u, c - base);
-#pragma unroll
-                        for(int k = 0; k < 32; ++k) {
-                            const float e = __shfl_sync(kFull, cur, k);
-                            if((uint32_t) k < m) ns = __fadd_rn(ns, e);
-                        }
+                    const uint32_t c4 = c & ~3u;
+#pragma unroll 8
+                    for(uint32_t i = 0; i < c4; i += 4) {
+                        const float4 v = *reinterpret_cast<const float4 *>(ND + i);
+                        ns = __fadd_rn(__fadd_rn(__fadd_rn(__fadd_rn(ns, v.x), v.y), v.z), v.w);
                     }
+                    for(uint32_t i = c4; i < c; ++i) ns = __fadd_rn(ns, ND[i]);
                 } else {
                     for(uint32_t i = 0; i < c; ++i) ns = __double2float_rn(__dadd_rn((double) ns, U[i]));
                 }
                 if(lane == 0) cyc[5] += clock64() - f0;
+            }
+            cluster_wait();
+            if(warp == 0) {
                 const uint32_t nslot = Linear && !mv ? y : t + x;
                 if((unsigned) lane < K) cluster.map_shared_rank(S, (unsigned) lane)[nslot] = ns;
             }
             __syncthreads();   // the folded row sum is in this CTA's S
             if(timer) t_last = clock64();
         } else {
+            cluster_wait();
             if(timer) mark(3);
             // Row/column x get the new distances; logical 0's row/column move
             // into y.
