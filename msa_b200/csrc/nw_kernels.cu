@@ -347,11 +347,15 @@ struct JobView {
     const uint64_t *poff;
     const uint32_t *plp;
     const uint32_t *sorted;     // clean sequences, eff descending
-    const uint8_t *row_narrow;  // 16-bit lanes for rows pair k
+    const uint8_t *row_narrow;  // per rows pair k: kRowNarrow, and kRowQuad for the first of a stacked pair
     int32_t *out;
     uint32_t nclean;
     int32_t g;
 };
+
+// row_narrow flags: 16-bit lanes; rows pairs k and k + 1 stacked in one warp
+// (quad_task), their tasks all under k.
+constexpr uint8_t kRowNarrow = 1, kRowQuad = 2;
 
 struct BatchParams {
     JobView job;
@@ -422,9 +426,15 @@ __device__ __forceinline__ uint32_t prmt0(uint32_t w)
 // wholly inside or wholly past X2's profile.
 constexpr int kStageBatch = 4;
 
+// With msplit < 2R (16-bit lanes only), chunks m >= msplit (strip rows
+// 16 msplit and on) come from a second rows pair, (g1b, g2b) at their row
+// 16 (m - msplit): the stacked strip of quad_task.
 template <int R, bool kNarrow, bool kPack = true>
 __device__ __forceinline__ void stage_words(uint32_t *sprof, const int8_t *__restrict__ g1, uint32_t lp1,
-                                            const int8_t *__restrict__ g2, uint32_t lp2, int i0, int32_t gap = 0)
+                                            const int8_t *__restrict__ g2, uint32_t lp2, int i0, int32_t gap = 0,
+                                            const int8_t *__restrict__ g1b = nullptr, uint32_t lp1b = 0,
+                                            const int8_t *__restrict__ g2b = nullptr, uint32_t lp2b = 0,
+                                            int msplit = 1 << 30)
 {
     using L = Layout<R, kNarrow, kPack>;
     constexpr int SH = L::SH;
@@ -442,9 +452,16 @@ __device__ __forceinline__ void stage_words(uint32_t *sprof, const int8_t *__res
                 va[u] = vb[u] = make_uint4(0, 0, 0, 0);
                 if(c < TOTAL) {
                     const int b = c / CH, m = c - b * CH;
-                    va[u] = __ldg(reinterpret_cast<const uint4 *>(g1 + (size_t) b * lp1 + i0) + m);
-                    if((uint32_t) (i0 + 16 * m) < lp2)
-                        vb[u] = __ldg(reinterpret_cast<const uint4 *>(g2 + (size_t) b * lp2 + i0) + m);
+                    if(m < msplit) {
+                        va[u] = __ldg(reinterpret_cast<const uint4 *>(g1 + (size_t) b * lp1 + i0) + m);
+                        if((uint32_t) (i0 + 16 * m) < lp2)
+                            vb[u] = __ldg(reinterpret_cast<const uint4 *>(g2 + (size_t) b * lp2 + i0) + m);
+                    } else {
+                        const int mb = m - msplit;
+                        va[u] = __ldg(reinterpret_cast<const uint4 *>(g1b + (size_t) b * lp1b) + mb);
+                        if((uint32_t) (16 * mb) < lp2b)
+                            vb[u] = __ldg(reinterpret_cast<const uint4 *>(g2b + (size_t) b * lp2b) + mb);
+                    }
                 }
             }
 #pragma unroll
@@ -517,6 +534,15 @@ __device__ __forceinline__ void stage_words(uint32_t *sprof, const int8_t *__res
 
 template <bool V> struct Guard { static constexpr bool value = V; };
 
+// Where the row above a strip comes from (sweep_strip's kTop):
+//   kTopBound  the boundary row in `bound` (any strip; the last row is stored
+//              back when store_bound);
+//   kTopZero   row zero of the gap-free state, 0, above lane 0 (a strip that
+//              is the first and the last one, 16-bit lanes only);
+//   kTopStack  as kTopZero, and lanes 16..31 hold a second rows pair of its
+//              own whose row zero sits above lane 16 (see quad_task).
+constexpr int kTopBound = 0, kTopZero = 1, kTopStack = 2;
+
 // Sweeps one strip (rows [i0, i0 + 32R)) of one column sequence on the calling
 // warp. `bound` holds the row above the strip on entry (column j at index j)
 // and, when store_bound, the strip's last row on exit. After the call, lane k's
@@ -524,7 +550,7 @@ template <bool V> struct Guard { static constexpr bool value = V; };
 // (tend - 1 - lane). Steps run in groups of 8 (the loop bookkeeping of a group
 // is shared by 8 columns); only the fill and drain groups, where some lanes
 // sit outside [0, ncols), test the lane's column.
-template <int R, class K, bool kPack = true>
+template <int R, class K, bool kPack = true, int kTop = kTopBound>
 __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, const uint8_t *__restrict__ cols,
                                             int ncols, uint32_t *__restrict__ bound, int i0, int tend,
                                             bool store_bound, int32_t g, int lane, typename K::W (&H)[R])
@@ -545,7 +571,12 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
         diag = K::splat(-(i0 + lane * R) * g);
     }
     W hlast = H[R - 1];
-    uint32_t bq_cur = bound[lane], bq_nxt = bound[32 + lane];
+    static_assert(kTop == kTopBound || kB, "row zero is 0 only in the gap-free 16-bit state");
+    uint32_t bq_cur = 0, bq_nxt = 0;
+    if constexpr(kTop == kTopBound) {
+        bq_cur = bound[lane];
+        bq_nxt = bound[32 + lane];
+    }
     const uint32_t *prow = sprof + lane * 4;
     const int half_off = L::HALF - lane * 2;      // the 16-bit half plane, from prow
     const int phalf_off = L::PHALF - lane * 2;    // the packed half plane, from prow
@@ -555,15 +586,21 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
 
     auto group = [&](int t0, auto guard) {
         constexpr bool kG = decltype(guard)::value;
-        if((t0 & 31) == 0 && t0 > 0) {
+        if(kTop == kTopBound && (t0 & 31) == 0 && t0 > 0) {
             bq_cur = bq_nxt;
             bq_nxt = bound[t0 + 32 + lane];
         }
 #pragma unroll
         for(int u = 0; u < 8; ++u) {
             W up = __shfl_up_sync(kFull, hlast, 1);
-            const uint32_t bv = __shfl_sync(kFull, bq_cur, (t0 & 31) + u);
-            if(lane == 0) up = (W) bv;
+            if constexpr(kTop == kTopBound) {
+                const uint32_t bv = __shfl_sync(kFull, bq_cur, (t0 & 31) + u);
+                if(lane == 0) up = (W) bv;
+            } else if constexpr(kTop == kTopZero) {
+                if(lane == 0) up = 0u;
+            } else {
+                if((lane & 15) == 0) up = 0u;
+            }
             if(!kG || (unsigned) j < (unsigned) ncols) {
                 const uint32_t *pb = prow + cur * SH;
                 W sc[4];
@@ -626,7 +663,8 @@ __device__ __forceinline__ void sweep_strip(const uint32_t *__restrict__ sprof, 
                 }
                 }
                 hlast = H[R - 1];
-                if(st31) bound[j] = (uint32_t) hlast;
+                if constexpr(kTop == kTopBound)
+                    if(st31) bound[j] = (uint32_t) hlast;
                 diag = up;
             }
             cur = nxt;
@@ -682,8 +720,9 @@ __device__ __noinline__ void narrow_task(uint32_t *sprof, const int8_t *g1, uint
         const uint32_t y = has ? jv.sorted[b] : tc.x1;
         const int ncols = has ? (int) jv.eff[y] : 0;
         const uint8_t *cols = jv.units + jv.uoff[y];
-        // Row zero of the DP (0 in the T state) as the boundary above the first strip.
-        if(has) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = 0u;
+        // Row zero of the DP (0 in the T state) as the boundary above the
+        // first of several strips (a single strip takes it as a constant).
+        if(has && nst > 1) for(int jj = lane; jj < ncols + 96; jj += 32) bound[jj] = 0u;
         int32_t r1 = 0, r2 = 0;
         for(int s = 0; s < nst; ++s) {
             const int i0 = s * SH;
@@ -697,7 +736,10 @@ __device__ __noinline__ void narrow_task(uint32_t *sprof, const int8_t *g1, uint
                 const int k1 = last ? (e1 - 1 - i0) / R : 31;
                 Narrow::W H[R];
                 __syncwarp();
-                sweep_strip<R, Narrow, kPack>(sprof, cols, ncols, bound, i0, ncols + k1, !last, g, lane, H);
+                if(nst == 1)
+                    sweep_strip<R, Narrow, kPack, kTopZero>(sprof, cols, ncols, bound, i0, ncols + k1, false, g, lane, H);
+                else
+                    sweep_strip<R, Narrow, kPack>(sprof, cols, ncols, bound, i0, ncols + k1, !last, g, lane, H);
                 __syncwarp();
                 if(s == s2) {
                     const int rr = e2 - 1 - i0;
@@ -758,6 +800,58 @@ __device__ __noinline__ void wide_task(uint32_t *sprof, const int8_t *g1, uint32
     }
 }
 
+// Two short rows pairs in one warp: pair A (sorted 2k, 2k+1) on lanes 0..15
+// and pair B (sorted 2k+2, 2k+3) on lanes 16..31, R rows per lane, so each
+// pair has 16R >= its rows in one strip; both sweep the same column
+// sequences (those of pair A: sorted 2k+1 + q W + warp). In the gap-free
+// state row zero is 0, so lane 16 takes 0 from above instead of lane 15's
+// last row, and the two halves never mix. A column is scored for a rows
+// sequence only when it comes after it in the sorted order. Halves the
+// per-step overhead per cell against a 16R-row strip on 32 lanes.
+template <int R, bool kPack>
+__device__ __noinline__ void quad_task(uint32_t *sprof, const JobView &jv, uint32_t k, uint32_t b0, uint32_t bstep,
+                                       uint32_t ngrp, int32_t g, int lane)
+{
+    const uint32_t xa1 = jv.sorted[2 * k], xa2 = jv.sorted[2 * k + 1];
+    const uint32_t xb1 = jv.sorted[2 * k + 2], xb2 = jv.sorted[2 * k + 3];
+    const int ea1 = (int) jv.eff[xa1], ea2 = (int) jv.eff[xa2], eb1 = (int) jv.eff[xb1], eb2 = (int) jv.eff[xb2];
+    for(uint32_t t = 0; t < ngrp; ++t) {
+        const uint32_t b = b0 + t * bstep;
+        const bool has = b < jv.nclean;
+        const uint32_t y = has ? jv.sorted[b] : xa1;
+        const int ncols = has ? (int) jv.eff[y] : 0;
+        const uint8_t *cols = jv.units + jv.uoff[y];
+        if(t == 0) {
+            __syncthreads();
+            stage_words<R, true, kPack>(sprof, jv.prof + jv.poff[xa1], jv.plp[xa1], jv.prof + jv.poff[xa2],
+                                        jv.plp[xa2], 0, g, jv.prof + jv.poff[xb1], jv.plp[xb1],
+                                        jv.prof + jv.poff[xb2], jv.plp[xb2], R);
+            __syncthreads();
+        }
+        if(has) {
+            Narrow::W H[R];
+            __syncwarp();
+            // Lane 31 is the last one to reach a column (pair B's rows).
+            sweep_strip<R, Narrow, kPack, kTopStack>(sprof, cols, ncols, nullptr, 0, ncols + 31, false, g, lane, H);
+            __syncwarp();
+            auto take = [&](int rows, int lane0, bool hi) {
+                const int rr = rows - 1;
+                const Narrow::W w = pick_row<R, Narrow>(H, rr % R);
+                const int32_t v = hi ? Narrow::hi(w, g, rows, ncols) : Narrow::lo(w, g, rows, ncols);
+                return __shfl_sync(kFull, v, lane0 + rr / R);
+            };
+            const int32_t ra1 = take(ea1, 0, false), ra2 = take(ea2, 0, true);
+            const int32_t rb1 = take(eb1, 16, false), rb2 = take(eb2, 16, true);
+            if(lane == 0) {
+                jv.out[tri_index(xa1, y)] = ra1;
+                if(b > 2 * k + 1) jv.out[tri_index(xa2, y)] = ra2;
+                if(b > 2 * k + 2) jv.out[tri_index(xb1, y)] = rb1;
+                if(b > 2 * k + 3) jv.out[tri_index(xb2, y)] = rb2;
+            }
+        }
+    }
+}
+
 // Strip plan for `rows` rows with at most 32*RMAX rows per strip: the fewest
 // strips, each of 32R rows with R the smallest even number that covers them.
 template <int RMAX>
@@ -794,6 +888,22 @@ __device__ __forceinline__ void rows_pair_task(const JobView &jv, uint32_t k, ui
     const int e1 = (int) jv.eff[x1], e2 = (int) jv.eff[x2];
     dev::TaskCols tc{&jv, x1, x2, a2, 2 * k + 1 + grp * W + warp, (uint32_t) W, ngrp};
 
+    if constexpr(RMAX == 32) {
+        if(jv.row_narrow[k] & kRowQuad) {
+            // Rows pairs k and k + 1 stacked (quad_task): R rows per lane, 16R
+            // covering pair k's longer first sequence.
+            int R = (e1 + 15) / 16;
+            R = (R + 1) & ~1;
+#define MSA_QUAD(RR) case RR: dev::quad_task<RR, kPack>(sprof_b, jv, k, tc.b0, tc.bstep, ngrp, jv.g, lane); break;
+            switch(R) {
+                MSA_QUAD(2) MSA_QUAD(4) MSA_QUAD(6) MSA_QUAD(8) MSA_QUAD(10) MSA_QUAD(12) MSA_QUAD(14) MSA_QUAD(16)
+                MSA_QUAD(18) MSA_QUAD(20) MSA_QUAD(22) MSA_QUAD(24) MSA_QUAD(26) MSA_QUAD(28) MSA_QUAD(30)
+                MSA_QUAD(32) default: break;
+            }
+#undef MSA_QUAD
+            return;
+        }
+    }
     if(jv.row_narrow[k]) {
         int nst, R;
         dev::strip_plan<RMAX>(e1, nst, R);
@@ -1218,9 +1328,24 @@ static int build_plan(msa_ctx *ctx, SeqStore *st, const ExtTable &tbl, int mode,
             const int64_t rows_p = (int64_t) round_up(st->eff[st->clean_sorted[2 * k]], SH);
             const int64_t cols = st->eff[st->clean_sorted[2 * k + 1]];
             const bool nar = narrow_ok(rows_p, cols, tbl) && !(ctx->nw_variant & MSA_NW_VARIANT_INT32);
-            row_narrow[k] = nar ? 1 : 0;
+            row_narrow[k] = nar ? kRowNarrow : 0;
             groups_k[k] = (uint64_t) (ncol + tiles.W - 1) / tiles.W;
             if(nar && k >= k_lo && k < k_hi) pl->narrow_tasks += (uint32_t) groups_k[k];
+        }
+        // Short rows pairs two by two in one warp (quad_task): both on 16-bit
+        // lanes with the state bound holding for 512 rows, the first's
+        // longer sequence within 16 x 32 rows, the second with two sequences
+        // and columns, and both in this part. The second's tasks are the
+        // first's.
+        if(tiles.R == 32 && narrow_ok(512, 512, tbl)) {
+            for(uint32_t k = k_lo; k + 1 < k_hi; ++k) {
+                if(!(row_narrow[k] && row_narrow[k + 1])) continue;
+                if(st->eff[st->clean_sorted[2 * k]] > 16 * 32) continue;
+                if(2 * (uint64_t) k + 3 >= nclean) break;
+                row_narrow[k] |= kRowQuad;
+                groups_k[k + 1] = 0;
+                ++k;
+            }
         }
         // Tasks of a single-strip rows pair take up to gchunk column groups
         // (one staging of the strip for all of them) while this part keeps at

@@ -54,6 +54,8 @@ def test_edge_sets_match_reference(gpu, golden, mode):
     (43, 9, 1500, 2600, "pam250"),      # several strips, wide columns
     (44, 33, 500, 530, "blosum45"),     # odd count: unpaired 16-bit task
     (45, 6, 5000, 7000, "blosum62"),    # 32-bit path (16-bit bound exceeded)
+    (46, 51, 300, 560, "blosum62"),     # stacked rows pairs (rows <= 512) beside single ones
+    (47, 20, 1, 512, "blosum90"),       # stacked rows pairs of every strip height
 ])
 def test_random_sets_match_oracle(gpu, tables, mode, seed, n, lo, hi, table):
     alpha = b"ACGTN" if table == "default" else b"ARNDCQEGHILKMFPSTWYV"
