@@ -830,7 +830,7 @@ def main():
     ap.add_argument("--arrival-seeds", default="5,6,7", help="with --sweep-windows: Poisson arrival seeds")
     ap.add_argument("--sweep-age", default="",
                     help="with --serve: comma-separated age weights (ms) of continuous admission to sweep instead")
-    ap.add_argument("--age-ms", type=float, default=10.0,
+    ap.add_argument("--age-ms", type=float, default=3.0,
                     help="with --serve: age weight (ms) of the age-weighted continuous run (0: skip it)")
     ap.add_argument("--window-ms", type=float, default=60.0,
                     help="with --serve: batch window of the headline serving run (0: continuous admission only)")
