@@ -305,8 +305,23 @@ typedef struct msa_nj_stats {
     uint32_t cluster;
     uint64_t cycles_scan, cycles_wait, cycles_join, cycles_join_wait, cycles_write;
     uint64_t cycles_fold, cycles_fold_row, cycles_fold_wait;
+    uint32_t helper_clusters;   /* clusters that scanned beside the joining one */
 } msa_nj_stats;
 int msa_nj_last_stats(const msa_ctx *ctx, msa_nj_stats *out);
+
+/* How a neighbor-joining run spreads its search over the GPU (no counterpart
+ * in the reference). One thread-block cluster makes every join; up to
+ * `clusters` - 1 more clusters (0 = the default, which is none; 1 = none)
+ * scan a share of the rows for each join while more than `helper_min_count`
+ * OTUs remain (0 = the default, 1,400), exchanging candidates and row sums
+ * through global memory; at most as many as are resident and 128 CTAs. Every
+ * wait between clusters ends after `wait_limit_us` (0 = the default, 1 s);
+ * a wait that runs out fails the call with MSA_ERR_DEVICE_TIMEOUT and leaves
+ * the context usable. `stall_publication` != 0 is a test hook: the joining
+ * cluster then never hands its row sums to the helpers, so their waits run
+ * out. Trees are the same under every setting. Applies to later calls. */
+int msa_nj_set_clusters(msa_ctx *ctx, int clusters, uint32_t helper_min_count, uint32_t wait_limit_us,
+                        int stall_publication);
 
 /* ---------------------------------------------------------------- serving */
 

@@ -69,7 +69,7 @@ class MsaNjStats(ctypes.Structure):
                 ("cluster", ctypes.c_uint32), ("cycles_scan", ctypes.c_uint64), ("cycles_wait", ctypes.c_uint64),
                 ("cycles_join", ctypes.c_uint64), ("cycles_join_wait", ctypes.c_uint64), ("cycles_write", ctypes.c_uint64),
                 ("cycles_fold", ctypes.c_uint64), ("cycles_fold_row", ctypes.c_uint64),
-                ("cycles_fold_wait", ctypes.c_uint64)]
+                ("cycles_fold_wait", ctypes.c_uint64), ("helper_clusters", ctypes.c_uint32)]
 
 
 class MsaServeConfig(ctypes.Structure):
@@ -143,6 +143,8 @@ _PROTOS = [
     ("msa_nj_order", ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_int,
                                     ctypes.POINTER(MsaOtu)]),
     ("msa_nj_last_stats", ctypes.c_int, [ctypes.c_void_p, ctypes.POINTER(MsaNjStats)]),
+    ("msa_nj_set_clusters", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_uint32, ctypes.c_uint32,
+                                           ctypes.c_int]),
     ("msa_probe_op", ctypes.c_int, [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.POINTER(MsaOpProbe)]),
     ("msa_serve_start", ctypes.c_int, [ctypes.POINTER(MsaServeConfig), ctypes.POINTER(ctypes.c_void_p)]),
     ("msa_serve_submit", ctypes.c_int, [ctypes.c_void_p, c_u8p, c_u64p, c_u64p, ctypes.c_uint32,

@@ -431,6 +431,17 @@ int msa_nw_last_stats(const msa_ctx *ctx, msa_nw_stats *out)
     return MSA_OK;
 }
 
+int msa_nj_set_clusters(msa_ctx *ctx, int clusters, uint32_t helper_min_count, uint32_t wait_limit_us,
+                        int stall_publication)
+{
+    if(!ctx || clusters < 0 || clusters > 9) return MSA_ERR_INVALID;
+    ctx->nj_clusters = clusters;
+    ctx->nj_helper_c = helper_min_count;
+    ctx->nj_wait_us = wait_limit_us;
+    ctx->nj_stall = stall_publication ? 1 : 0;
+    return MSA_OK;
+}
+
 int msa_nj_last_stats(const msa_ctx *ctx, msa_nj_stats *out)
 {
     if(!ctx || !out) return MSA_ERR_INVALID;

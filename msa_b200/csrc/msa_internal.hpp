@@ -112,6 +112,12 @@ struct msa_ctx {
     int tile_r = 0, tile_w = 0;   // persistent-kernel tile override (0 = autotuned)
     int nw_variant = 0;           // msa_nw_set_variant flags (0 = the committed kernel)
     uint32_t nw_chunk = 0;        // column groups per single-strip task (0 = autotuned)
+    // msa_nj_set_clusters: clusters of the NJ launch (0 = automatic, 1 = one),
+    // OTU count above which helpers scan (0 = default), wait limit between
+    // clusters in microseconds (0 = default), and the stalled-publication test hook.
+    int nj_clusters = 0;
+    uint32_t nj_helper_c = 0, nj_wait_us = 0;
+    int nj_stall = 0;
 };
 
 namespace msa {

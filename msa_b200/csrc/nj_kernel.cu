@@ -101,12 +101,297 @@ struct State {
     const float *S0;           // initial row sums by slot
     uint32_t *rec_x, *rec_y;   // logical indices joined at each step
     float *rec_dx, *rec_dy;
-    int *err;
+    int *err;                  // 2: no joinable pair; 3: a wait between clusters ran out; 4: an invalid pair
     unsigned long long *cycles;   // kCycleSlots phase counters
     uint32_t n, P;
+    // Helper clusters (clusters 1.. of the launch) scan a share of the rows
+    // while the OTU count exceeds helper_c; cluster 0 joins. Zero-filled
+    // before the launch.
+    uint32_t helper_ctas;      // CTAs of all helper clusters (0: cluster 0 alone)
+    uint32_t helper_c;
+    float *s_pub;              // [2][P] row sums published by the folding CTA after a join
+    uint32_t *pub_xy;          // [2] the join (x << 16 | y) they follow
+    uint32_t *pub_seq;         // join number + 1 of the last publication; kStop ends the helpers
+    unsigned long long *cand;  // [2][helper_ctas][2] each helper CTA's candidate (key, x << 16 | y)
+    uint32_t *cand_seq;        // [helper_ctas] join number + 1 of its last candidate
+    unsigned long long wait_ns;   // limit of every wait between clusters
+    int stall_publication;     // test hook: the folding CTA never publishes
 };
 
+constexpr uint32_t kStop = 0xffffffffu;
+// Helper clusters: at most this many CTAs in all; kDefaultClusters - 1 of
+// them by default (none: on 2,000 OTUs, 3 helper clusters above 1,400 OTUs
+// measured 21.65 ms against 21.64 ms for one cluster, because the two
+// handoffs through global memory per join cost what the wider scan saves),
+// scanning while more than kHelperMinCount OTUs remain; every wait between
+// clusters ends after kWaitUs.
+constexpr uint32_t kMaxHelperCtas = 128;
+constexpr uint32_t kDefaultClusters = 1;
+constexpr uint32_t kHelperMinCount = 1400;
+constexpr uint32_t kWaitUs = 1000000;
+
+// Release/acquire flags between clusters (gpu scope) and the global timer
+// that bounds every wait on them.
+__device__ __forceinline__ uint32_t ld_acquire(const uint32_t *p)
+{
+    uint32_t v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release(uint32_t *p, uint32_t v)
+{
+    asm volatile("st.release.gpu.global.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ unsigned long long global_ns()
+{
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// Waits until *flag >= want; returns the value seen, or 0 when `limit_ns`
+// passed first (the caller reports the timeout and stops waiting).
+__device__ __forceinline__ uint32_t wait_flag(const uint32_t *flag, uint32_t want, unsigned long long limit_ns)
+{
+    const unsigned long long t0 = global_ns();
+    for(;;) {
+        const uint32_t v = ld_acquire(flag);
+        if(v >= want) return v;
+        if(global_ns() - t0 > limit_ns) return 0u;
+        __nanosleep(128);
+    }
+}
+
+// One scanning warp's share of a join's search (the kernel's scan phase):
+// rows i = c-1 down to 1 of the logical lower triangle, longest first, warp
+// gw of W taking places gw and 2W-1-gw of every 2W, so long and short rows
+// pair up and the last, partial 2W hold the shortest rows. Warp `warp` of
+// scanning CTA `s` (of `ns`) is gw = warp * ns + s, so consecutive places
+// fall in different CTAs and the partial block spreads over all of them
+// (with rows ascending and gw = s * 32 + warp, the longest leftover rows all
+// fell to the first CTAs). The CTA's copy of
+// S holds +inf in the dropped slots (< t) and in `moved`'s slot, so those
+// columns give Q = -inf or NaN and never win; the new node's column and the
+// cells past a row's end are masked. Each lane keeps, per row, the largest
+// chunk maximum and the first chunk reaching it, and its best over rows by
+// (Q, row, chunk), which orders like the row-major index; the element inside
+// the winning chunk is resolved once, after the scan. `moved`'s column of
+// later rows is read from where its data still is (slot mslot): lane r loads
+// it for the warp's r-th row before the row loop and offers it after, so the
+// load waits in the shadow of the scan. The lane's best candidate goes into
+// (best, best_xy).
+struct ScanView {
+    const float *D;   // slot t + k holds logical k; row pitch P
+    const float *S;   // this CTA's row sums by slot
+    uint32_t P, t, c, pend, moved, mslot;
+    float cm2, s_moved;
+};
+
+__device__ __forceinline__ void scan_rows(const ScanView &v, uint32_t s, uint32_t ns, int warp, int lane,
+                                          unsigned long long &best, uint32_t &best_xy)
+{
+    const uint32_t W = ns * kWarps, gw = (uint32_t) warp * ns + s;
+    auto offer = [&](unsigned long long q, uint32_t i, uint32_t j) {
+        if(q > best) {
+            best = q;
+            best_xy = (i << 16) | j;
+        }
+    };
+    const uint32_t skip1 = v.pend == kNone ? kNone : v.t + v.pend;
+    const uint32_t base4 = v.t & ~3u;
+    const float s_moved = v.s_moved;
+    auto row_of = [&](uint32_t i) { return v.D + (size_t) (i == v.moved ? v.mslot : v.t + i) * v.P + base4; };
+    auto chunk_q = [&](const float4 &d, uint32_t col, uint32_t hi, float si, float &q0, float &q1, float &q2,
+                       float &q3) {
+        const float4 s = *reinterpret_cast<const float4 *>(v.S + col);
+        q0 = __fsub_rn(__fsub_rn(__fmul_rn(v.cm2, d.x), si), s.x);
+        q1 = __fsub_rn(__fsub_rn(__fmul_rn(v.cm2, d.y), si), s.y);
+        q2 = __fsub_rn(__fsub_rn(__fmul_rn(v.cm2, d.z), si), s.z);
+        q3 = __fsub_rn(__fsub_rn(__fmul_rn(v.cm2, d.w), si), s.w);
+        if(col + 4 > hi || skip1 - col < 4u) {
+            if(col >= hi || col == skip1) q0 = -INFINITY;
+            if(col + 1 >= hi || col + 1 == skip1) q1 = -INFINITY;
+            if(col + 2 >= hi || col + 2 == skip1) q2 = -INFINITY;
+            if(col + 3 >= hi || col + 3 == skip1) q3 = -INFINITY;
+        }
+    };
+    // The row of the warp's place p (p = 0 is row c-1), or 0 past the end.
+    auto row_at = [&](uint32_t p) { return p + 1 < v.c ? v.c - 1 - p : 0u; };
+    // The warp's r-th row (r = 2 * block + half), 0 when it has none or when
+    // column `v.moved` of it is not read here.
+    auto moved_row = [&](uint32_t r) {
+        const uint32_t i = row_at((r >> 1) * 2 * W + ((r & 1) ? 2 * W - 1 - gw : gw));
+        return (i <= v.moved || i == v.pend) ? 0u : i;
+    };
+    // Column `v.moved` of the warp's r-th row, for r = lane (with 15 scanning
+    // CTAs a warp has at most 2 * ceil(12800 / 960) = 28 rows; any beyond 32
+    // are read after the scan), from where logical 0's data still is.
+    uint32_t mi = 0;
+    float mq = 0.0f;
+    if(v.moved != kNone) {
+        mi = moved_row((uint32_t) lane);
+        if(mi) mq = __ldcg(v.D + (size_t) (v.t + mi) * v.P + v.mslot);
+    }
+    unsigned long long lbest = 0;   // (key << 32) | ~(row << 14 | chunk)
+    for(uint32_t base = 0; base + 1 < v.c; base += 2 * W) {
+#pragma unroll 1
+        for(int h = 0; h < 2; ++h) {
+            const uint32_t i = row_at(base + (h ? 2 * W - 1 - gw : gw));
+            if(i == 0 || i == v.pend) continue;
+            const uint32_t hi = v.t + i;
+            const float *row = row_of(i);
+            const float si = i == v.moved ? s_moved : v.S[v.t + i];
+            const uint32_t nch = (hi - base4 + 3) >> 2;
+            float bq = -INFINITY;
+            uint32_t bg = 0;
+            for(uint32_t g0 = lane; g0 < nch; g0 += 32 * kBatch) {
+                float4 d[kBatch];
+#pragma unroll
+                for(int u = 0; u < kBatch; ++u)
+                    if(g0 + 32 * u < nch) d[u] = __ldcg(reinterpret_cast<const float4 *>(row + 4 * (g0 + 32 * u)));
+#pragma unroll
+                for(int u = 0; u < kBatch; ++u) {
+                    const uint32_t g = g0 + 32 * u;
+                    if(g < nch) {
+                        float q0, q1, q2, q3;
+                        chunk_q(d[u], base4 + 4 * g, hi, si, q0, q1, q2, q3);
+                        const float m = fmaxf(fmaxf(q0, q1), fmaxf(q2, q3));
+                        if(m > bq) {
+                            bq = m;
+                            bg = g;
+                        }
+                    }
+                }
+            }
+            const uint32_t key = order_key(bq);
+            if(key) lbest = umax64(lbest, ((unsigned long long) key << 32) | (0xffffffffu - ((i << 14) | bg)));
+        }
+    }
+    if(v.moved != kNone) {
+        const uint32_t rows = 2 * ((v.c - 1 + 2 * W - 1) / (2 * W));
+        for(uint32_t r = (uint32_t) lane;;) {
+            if(mi) {
+                const float q = __fsub_rn(__fsub_rn(__fmul_rn(v.cm2, mq), v.S[v.t + mi]), s_moved);
+                offer(pack(order_key(q), mi * (mi - 1) / 2 + v.moved), mi, v.moved);
+            }
+            r += 32;
+            if(r >= rows) break;
+            mi = moved_row(r);
+            if(mi) mq = __ldcg(v.D + (size_t) (v.t + mi) * v.P + v.mslot);
+        }
+    }
+    if(lbest) {
+        const uint32_t tail = 0xffffffffu - (uint32_t) (lbest & 0xffffffffull);
+        const uint32_t i = tail >> 14, g = tail & 0x3fffu, col = base4 + 4 * g;
+        const float si = i == v.moved ? s_moved : v.S[v.t + i];
+        float q[4];
+        chunk_q(__ldcg(reinterpret_cast<const float4 *>(row_of(i) + 4 * g)), col, v.t + i, si, q[0], q[1], q[2], q[3]);
+        const uint32_t key = (uint32_t) (lbest >> 32);
+        int k = 3;
+        if(order_key(q[2]) == key) k = 2;   // keep the first element equal to the maximum
+        if(order_key(q[1]) == key) k = 1;
+        if(order_key(q[0]) == key) k = 0;
+        const uint32_t j = col + k - v.t;
+        offer(pack(key, i * (i - 1) / 2 + j), i, j);
+    }
+}
+
+// A helper CTA (clusters 1.. of the launch): scans its share of the rows of
+// every join while the OTU count exceeds helper_c, with the same removal
+// bookkeeping as cluster 0, and hands its best candidate to cluster 0's CTA 0.
+// It starts from the initial row sums; after each join it takes the row sums
+// and the joined pair that the folding CTA publishes (double-buffered by
+// join parity) and masks them as the scanning CTAs of cluster 0 do. `sidx`
+// is its place among all scanning CTAs (cluster 0's come first), `nscan` the
+// number of them. Every wait is bounded by st.wait_ns; a wait
+// that runs out sets err = 3 and ends the helper.
 template <bool Linear>
+__device__ void nj_helper(const State &st, float *S, uint32_t hidx, uint32_t sidx, uint32_t nscan)
+{
+    __shared__ unsigned long long hbest[kWarps];
+    __shared__ uint32_t hxy[kWarps];
+    __shared__ float h_moved;
+    __shared__ int h_stop;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const uint32_t n = st.n, P = st.P;
+    for(uint32_t k = tid; k < P; k += kThreads) S[k] = k < n ? st.S0[k] : 0.0f;
+    if(tid == 0) {
+        h_moved = 0.0f;
+        h_stop = 0;
+    }
+    __syncthreads();
+    uint32_t c = n, t = 0, step = 0, pend = kNone, moved = kNone, mslot = 0;
+    while(c > 1 && c > st.helper_c) {
+        unsigned long long best = 0;
+        uint32_t best_xy = 0;
+        scan_rows(ScanView{st.D, S, P, t, c, pend, moved, mslot, (float) (c - 2), h_moved}, sidx, nscan, warp, lane,
+                  best, best_xy);
+        {
+            const unsigned long long wm = warp_max(best);
+            if(best == wm && wm != 0ull) hxy[warp] = best_xy;
+            if(lane == 0) hbest[warp] = wm;
+        }
+        __syncthreads();
+        const uint32_t buf = step & 1u;
+        if(warp == 0) {
+            const unsigned long long v = lane < kWarps ? hbest[lane] : 0ull;
+            const unsigned long long m = warp_max(v);
+            const uint32_t holder = __ffs(__ballot_sync(kFull, v == m)) - 1;
+            if(lane == 0) {
+                unsigned long long *slot = st.cand + ((size_t) buf * st.helper_ctas + hidx) * 2;
+                slot[0] = m;
+                slot[1] = m ? hxy[holder] : 0u;
+                st_release(st.cand_seq + hidx, step + 1);
+            }
+        }
+        if(c - 1 <= st.helper_c) break;   // cluster 0 scans the next joins alone
+        if(tid == 0) {
+            const uint32_t v = wait_flag(st.pub_seq, step + 1, st.wait_ns);
+            if(v == 0u) atomicExch(st.err, 3);
+            h_stop = (v == 0u || v == kStop) ? 1 : 0;
+        }
+        __syncthreads();
+        if(h_stop) break;
+        // The join cluster 0 made, and its row sums after it.
+        const uint32_t xy = __ldcg(st.pub_xy + buf);
+        const uint32_t x = xy >> 16, y = xy & 0xffffu;
+        if(x >= c || y >= x) {   // never a pair of this join
+            if(tid == 0) atomicExch(st.err, 4);
+            break;
+        }
+        const float *pub = st.s_pub + (size_t) buf * P;
+        // Slots [t, t + c) only: those below t were dropped and keep the +inf
+        // that masks them in the scan's first chunk (from slot t & ~3).
+        for(uint32_t k = t + tid; k < t + c; k += kThreads) S[k] = __ldcg(pub + k);
+        __syncthreads();
+        const bool mv = Linear ? x != c - 1 : y != 0;
+        if(tid == 0) {
+            // As the scanning CTAs of cluster 0 (update_cache): the moved
+            // data's row sum aside, +inf in its slot and in a dropped slot.
+            if(mv) {
+                h_moved = S[t + y];
+                S[t + y] = INFINITY;
+            }
+            if(!Linear) S[t] = INFINITY;
+        }
+        if(Linear) {
+            pend = mv ? x : y;
+            moved = mv ? y : kNone;
+            mslot = c - 1;
+        } else {
+            pend = x - 1;
+            moved = y != 0 ? y - 1 : kNone;
+            mslot = t;
+            ++t;
+        }
+        ++step;
+        --c;
+        __syncthreads();
+    }
+}
+
+// kHelp: the launch has helper clusters (compiled separately, so that the
+// one-cluster kernel carries none of their code).
+template <bool Linear, bool kHelp>
 __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
 {
     cg::cluster_group cluster = cg::this_cluster();
@@ -130,12 +415,25 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
     const unsigned K = cluster.num_blocks();
     const unsigned rank = cluster.block_rank();
     const unsigned F = K - 1;   // the CTA that folds new row sums
+    if constexpr(kHelp) {
+        if(blockIdx.x >= K) {       // a helper cluster
+            nj_helper<Linear>(st, reinterpret_cast<float *>(smem_raw), blockIdx.x - K, F + blockIdx.x - K,
+                              F + st.helper_ctas);
+            return;
+        }
+    }
     const bool folder = rank == F;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     float *D = st.D;
+    // Set (in every CTA of cluster 0, before barrier A) once a wait for the
+    // helpers ran out: cluster 0 then scans alone.
+    __shared__ int hoff;
     const bool timer = tid == 0 && (rank == 0 || folder);
     if(tid < kCycleSlots) cyc[tid] = 0;
-    if(tid == 0) s_moved_sh = 0.0f;
+    if(tid == 0) {
+        s_moved_sh = 0.0f;
+        hoff = 0;
+    }
     unsigned long long t_last = clock64();
     auto mark = [&](int k) {
         const unsigned long long now = clock64();
@@ -158,10 +456,12 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
     // of every later row.
     // `mslot` is the slot where `moved`'s data still is.
     uint32_t pend = kNone, moved = kNone, mslot = 0;
-    bool failed = false;
+    bool failed = false, bad = false;
 
     while(c > 1) {
         const float cm2 = (float) (c - 2);
+        // The helper clusters scan with cluster 0 for this join.
+        const bool helped = kHelp && st.helper_ctas != 0u && !hoff && c > st.helper_c;
         unsigned long long best = 0;
         uint32_t best_xy = 0;
         auto offer = [&](unsigned long long v, uint32_t i, uint32_t j) {
@@ -182,81 +482,8 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             // the first chunk reaching it, and its best over rows by (Q, row,
             // chunk), which orders like the row-major index; the element
             // inside the winning chunk is resolved once, after the scan.
-            const uint32_t W = F * kWarps;
-            const uint32_t gw = rank * kWarps + warp;
-            const uint32_t skip1 = pend == kNone ? kNone : t + pend;
-            const uint32_t base4 = t & ~3u;
-            const float s_moved = s_moved_sh;
-            auto row_of = [&](uint32_t i) { return D + (size_t) (i == moved ? mslot : t + i) * P + base4; };
-            auto chunk_q = [&](const float4 &d, uint32_t col, uint32_t hi, float si, float &q0, float &q1, float &q2,
-                               float &q3) {
-                const float4 s = *reinterpret_cast<const float4 *>(S + col);
-                q0 = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d.x), si), s.x);
-                q1 = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d.y), si), s.y);
-                q2 = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d.z), si), s.z);
-                q3 = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d.w), si), s.w);
-                if(col + 4 > hi || skip1 - col < 4u) {
-                    if(col >= hi || col == skip1) q0 = -INFINITY;
-                    if(col + 1 >= hi || col + 1 == skip1) q1 = -INFINITY;
-                    if(col + 2 >= hi || col + 2 == skip1) q2 = -INFINITY;
-                    if(col + 3 >= hi || col + 3 == skip1) q3 = -INFINITY;
-                }
-            };
-            unsigned long long lbest = 0;   // (key << 32) | ~(row << 14 | chunk)
-            for(uint32_t base = 0; base + 1 < c; base += 2 * W) {
-#pragma unroll 1
-                for(int h = 0; h < 2; ++h) {
-                    const uint32_t i = base + 1 + (h ? 2 * W - 1 - gw : gw);
-                    if(i >= c || i == pend) continue;
-                    const uint32_t hi = t + i;
-                    const float *row = row_of(i);
-                    const float si = i == moved ? s_moved : S[t + i];
-                    const uint32_t nch = (hi - base4 + 3) >> 2;
-                    float bq = -INFINITY;
-                    uint32_t bg = 0;
-                    for(uint32_t g0 = lane; g0 < nch; g0 += 32 * kBatch) {
-                        float4 d[kBatch];
-#pragma unroll
-                        for(int u = 0; u < kBatch; ++u)
-                            if(g0 + 32 * u < nch) d[u] = __ldcg(reinterpret_cast<const float4 *>(row + 4 * (g0 + 32 * u)));
-#pragma unroll
-                        for(int u = 0; u < kBatch; ++u) {
-                            const uint32_t g = g0 + 32 * u;
-                            if(g < nch) {
-                                float q0, q1, q2, q3;
-                                chunk_q(d[u], base4 + 4 * g, hi, si, q0, q1, q2, q3);
-                                const float m = fmaxf(fmaxf(q0, q1), fmaxf(q2, q3));
-                                if(m > bq) {
-                                    bq = m;
-                                    bg = g;
-                                }
-                            }
-                        }
-                    }
-                    const uint32_t key = order_key(bq);
-                    if(key) lbest = umax64(lbest, ((unsigned long long) key << 32) | (0xffffffffu - ((i << 14) | bg)));
-                    // Column `moved` of a later row, from where logical 0's data still is.
-                    if(lane == 0 && moved != kNone && i > moved) {
-                        const float dm = __ldcg(D + (size_t) (t + i) * P + mslot);
-                        const float q = __fsub_rn(__fsub_rn(__fmul_rn(cm2, dm), si), s_moved);
-                        offer(pack(order_key(q), i * (i - 1) / 2 + moved), i, moved);
-                    }
-                }
-            }
-            if(lbest) {
-                const uint32_t tail = 0xffffffffu - (uint32_t) (lbest & 0xffffffffull);
-                const uint32_t i = tail >> 14, g = tail & 0x3fffu, col = base4 + 4 * g;
-                const float si = i == moved ? s_moved : S[t + i];
-                float q[4];
-                chunk_q(__ldcg(reinterpret_cast<const float4 *>(row_of(i) + 4 * g)), col, t + i, si, q[0], q[1], q[2], q[3]);
-                const uint32_t key = (uint32_t) (lbest >> 32);
-                int k = 3;
-                if(order_key(q[2]) == key) k = 2;   // keep the first element equal to the maximum
-                if(order_key(q[1]) == key) k = 1;
-                if(order_key(q[0]) == key) k = 0;
-                const uint32_t j = col + k - t;
-                offer(pack(key, i * (i - 1) / 2 + j), i, j);
-            }
+            scan_rows(ScanView{D, S, P, t, c, pend, moved, mslot, cm2, s_moved_sh}, rank,
+                      F + (helped ? st.helper_ctas : 0u), warp, lane, best, best_xy);
         } else if(pend != kNone) {
             // The new node's row and column, from the distances the last join
             // computed (ND, indexed by that join's logical order: logical j
@@ -288,12 +515,45 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
         __syncthreads();
         if(warp == 0) {
             const unsigned long long v = lane < kWarps ? wbest[lane] : 0ull;
-            const unsigned long long m = warp_max(v);
+            unsigned long long m = warp_max(v);
             const uint32_t holder = __ffs(__ballot_sync(kFull, v == m)) - 1;
-            const uint32_t xy = m ? wxy[holder] : 0u;
+            uint32_t xy = m ? wxy[holder] : 0u;
+            int off = 0;
+            if(kHelp && rank == 0 && helped) {
+                // The helper CTAs' candidates for this join, each lane waiting
+                // for its share of them; merged into this CTA's part.
+                const uint32_t buf = step & 1u;
+                unsigned long long hb = 0;
+                uint32_t hxyv = 0;
+                bool ok = true;
+                for(uint32_t h = lane; h < st.helper_ctas; h += 32) {
+                    if(ok && wait_flag(st.cand_seq + h, step + 1, st.wait_ns) != 0u) {
+                        const unsigned long long *slot = st.cand + ((size_t) buf * st.helper_ctas + h) * 2;
+                        const unsigned long long key = __ldcg(slot);
+                        if(key > hb) {
+                            hb = key;
+                            hxyv = (uint32_t) __ldcg(slot + 1);
+                        }
+                    } else {
+                        ok = false;
+                    }
+                }
+                const unsigned long long hm = warp_max(hb);
+                const uint32_t hh = __ffs(__ballot_sync(kFull, hb == hm)) - 1;
+                const uint32_t hmxy = __shfl_sync(kFull, hxyv, hh);
+                if(hm > m) {
+                    m = hm;
+                    xy = hmxy;
+                }
+                if(!__all_sync(kFull, ok)) {
+                    off = 1;
+                    if(lane == 0) atomicExch(st.err, 3);
+                }
+            }
             if((unsigned) lane < K) {
                 cluster.map_shared_rank(parts, (unsigned) lane)[rank] = m;
                 cluster.map_shared_rank(part_xy, (unsigned) lane)[rank] = xy;
+                if(off) cluster.map_shared_rank(&hoff, (unsigned) lane)[0] = 1;
             }
         }
         if(timer) mark(rank == 0 ? 0 : 6);
@@ -314,6 +574,10 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             break;
         }
         const uint32_t x = part_xy[wr] >> 16, y = part_xy[wr] & 0xffffu;
+        if(x >= c || y >= x) {   // never a pair of this join: report it, touch nothing
+            bad = true;
+            break;
+        }
         // The logical index whose data takes y's place (0, or the last in the
         // linear order), and whether there is such a move: none when y is 0
         // (symmetric), or when x itself is the last (linear; the new node then
@@ -399,6 +663,20 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
                     S[t + y] = INFINITY;
                 }
                 if(!Linear) S[t] = INFINITY;
+            }
+        }
+        // The row sums after this join and the joined pair, for the helper
+        // clusters' next scan (the folding CTA's copy has no +inf masks).
+        if(kHelp && folder && st.helper_ctas != 0u && !hoff && c - 1 > st.helper_c) {
+            __syncthreads();   // update_cache above
+            const uint32_t buf = step & 1u;
+            float *pub = st.s_pub + (size_t) buf * P;
+            for(uint32_t k = t + tid; k < t + c; k += kThreads) __stcg(pub + k, S[k]);
+            if(tid == 0) st.pub_xy[buf] = (x << 16) | y;
+            __syncthreads();
+            if(tid == 0 && !st.stall_publication) {
+                __threadfence();
+                st_release(st.pub_seq, step + 1);
             }
         }
         if(timer && rank == 0) mark(2);
@@ -518,6 +796,9 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
         --c;
     }
     if(failed && rank == 0 && tid == 0) atomicExch(st.err, 2);
+    if(bad && rank == 0 && tid == 0) atomicExch(st.err, 4);
+    // Helpers still waiting for a publication stop.
+    if(kHelp && folder && tid == 0 && st.helper_ctas != 0u && !st.stall_publication) st_release(st.pub_seq, kStop);
     if(tid == 0 && rank == 0)
         for(int k = 0; k < 5; ++k) st.cycles[k] = cyc[k];
     if(tid == 0 && folder)
@@ -556,7 +837,7 @@ __global__ void row_sums_kernel(const float *__restrict__ D, float *__restrict__
 
 // Largest cluster (16, 8, 4 or 2 CTAs) that can be resident with `smem` bytes
 // of dynamic shared memory per CTA; 0 if none.
-template <bool Linear>
+template <bool Linear, bool kHelp>
 unsigned pick_cluster(size_t smem)
 {
     for(unsigned k : {16u, 8u, 4u, 2u}) {
@@ -572,7 +853,8 @@ unsigned pick_cluster(size_t smem)
         cfg.attrs = attr;
         cfg.numAttrs = 1;
         int clusters = 0;
-        if(cudaOccupancyMaxActiveClusters(&clusters, nj_cluster_kernel<Linear>, &cfg) == cudaSuccess && clusters >= 1)
+        if(cudaOccupancyMaxActiveClusters(&clusters, nj_cluster_kernel<Linear, kHelp>, &cfg) == cudaSuccess &&
+           clusters >= 1)
             return k;
         cudaGetLastError();
     }
@@ -584,7 +866,8 @@ unsigned pick_cluster(size_t smem)
 int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, int order, msa_otu *out)
 {
     const bool linear = order == MSA_NJ_LINEAR;
-    auto kern = linear ? njdev::nj_cluster_kernel<true> : njdev::nj_cluster_kernel<false>;
+    auto kern_one = linear ? njdev::nj_cluster_kernel<true, false> : njdev::nj_cluster_kernel<false, false>;
+    auto kern_help = linear ? njdev::nj_cluster_kernel<true, true> : njdev::nj_cluster_kernel<false, true>;
     cudaStream_t s = ctx->stream;
     const uint32_t P = (n + 3) & ~3u;
     const size_t smem = (size_t) P * 16;   // S, ND (4 B each), U (8 B)
@@ -596,7 +879,11 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, int order, msa_o
     auto take = [&off](size_t b) { size_t o = off; off = round_up(off + b, 256); return o; };
     const size_t oD = take((size_t) n * P * 4), oS = take(n * 4), oRx = take(n * 4), oRy = take(n * 4),
                  oRdx = take(n * 4), oRdy = take(n * 4), oErr = take(64), oCyc = take(64),
-                 oTri = take((kind == MSA_TRI_F32_HOST || kind == MSA_TRI_I32_HOST) ? ntri * 4 : 0);
+                 oTri = take((kind == MSA_TRI_F32_HOST || kind == MSA_TRI_I32_HOST) ? ntri * 4 : 0),
+                 oPub = take((size_t) 2 * P * 4),
+                 // flags between clusters: pub_seq, pub_xy[2], cand_seq[], cand[][][2]
+                 oSync = take(64 + (size_t) njdev::kMaxHelperCtas * 4),
+                 oCand = take((size_t) 2 * njdev::kMaxHelperCtas * 16);
     MSA_CUDA_TRY(ctx, ctx->nj_buf.ensure(off));
     char *base = (char *) ctx->nj_buf.ptr;
     njdev::State st{};
@@ -611,10 +898,49 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, int order, msa_o
     st.n = n;
     st.P = P;
 
-    MSA_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
-    MSA_CUDA_TRY(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
-    const unsigned K = linear ? njdev::pick_cluster<true>(smem) : njdev::pick_cluster<false>(smem);
+    for(auto kf : {kern_one, kern_help}) {
+        MSA_CUDA_TRY(ctx, cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        MSA_CUDA_TRY(ctx, cudaFuncSetAttribute(kf, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    }
+    const unsigned K = linear ? njdev::pick_cluster<true, false>(smem) : njdev::pick_cluster<false, false>(smem);
     if(K < 2) return set_error(ctx, MSA_ERR_CUDA, "neighbor-joining cluster cannot be resident");
+    // Helper clusters: as many as can be resident beside cluster 0 (each on
+    // its own GPC), at most the context's setting, and only when some join
+    // has more OTUs than the helpers' threshold.
+    const uint32_t helper_c = std::max<uint32_t>(ctx->nj_helper_c ? ctx->nj_helper_c : njdev::kHelperMinCount, 2);
+    uint32_t clusters = 1;
+    if(ctx->nj_clusters != 1 && n > helper_c + 1) {
+        cudaLaunchConfig_t q = {};
+        cudaLaunchAttribute qa[1];
+        qa[0].id = cudaLaunchAttributeClusterDimension;
+        qa[0].val.clusterDim.x = K;
+        qa[0].val.clusterDim.y = 1;
+        qa[0].val.clusterDim.z = 1;
+        q.gridDim = dim3(K);
+        q.blockDim = dim3(njdev::kThreads);
+        q.dynamicSmemBytes = smem;
+        q.attrs = qa;
+        q.numAttrs = 1;
+        int resident = 0;
+        if(cudaOccupancyMaxActiveClusters(&resident, kern_help, &q) != cudaSuccess) {
+            cudaGetLastError();
+            resident = 1;
+        }
+        const uint32_t want = ctx->nj_clusters ? (uint32_t) ctx->nj_clusters : njdev::kDefaultClusters;
+        clusters = std::max<uint32_t>(1, std::min<uint32_t>({want, (uint32_t) resident,
+                                                              1 + njdev::kMaxHelperCtas / K}));
+    }
+    auto kern = clusters > 1 ? kern_help : kern_one;
+    char *sync = base + oSync;
+    st.helper_ctas = (clusters - 1) * K;
+    st.helper_c = helper_c;
+    st.s_pub = (float *) (base + oPub);
+    st.pub_seq = (uint32_t *) sync;
+    st.pub_xy = (uint32_t *) (sync + 16);
+    st.cand_seq = (uint32_t *) (sync + 64);
+    st.cand = (unsigned long long *) (base + oCand);
+    st.wait_ns = (unsigned long long) (ctx->nj_wait_us ? ctx->nj_wait_us : njdev::kWaitUs) * 1000ull;
+    st.stall_publication = ctx->nj_stall;
 
     MSA_CUDA_TRY(ctx, cudaEventRecord(ctx->ev[0], s));
     const void *dtri = tri;
@@ -632,6 +958,7 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, int order, msa_o
     MSA_CUDA_TRY(ctx, cudaGetLastError());
     MSA_CUDA_TRY(ctx, cudaMemsetAsync(base + oErr, 0, 64, s));
     MSA_CUDA_TRY(ctx, cudaMemsetAsync(base + oCyc, 0, 64, s));
+    MSA_CUDA_TRY(ctx, cudaMemsetAsync(sync, 0, 64 + (size_t) njdev::kMaxHelperCtas * 4, s));
     ctx->launches += 2;
 
     cudaLaunchConfig_t cfg = {};
@@ -640,7 +967,7 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, int order, msa_o
     attr[0].val.clusterDim.x = K;
     attr[0].val.clusterDim.y = 1;
     attr[0].val.clusterDim.z = 1;
-    cfg.gridDim = dim3(K);
+    cfg.gridDim = dim3(K * clusters);
     cfg.blockDim = dim3(njdev::kThreads);
     cfg.dynamicSmemBytes = smem;
     cfg.stream = s;
@@ -671,6 +998,7 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, int order, msa_o
         ns.total_ms = ms_all;
         ns.n = n;
         ns.cluster = K;
+        ns.helper_clusters = clusters - 1;
         ns.cycles_scan = cyc[0];
         ns.cycles_wait = cyc[1];
         ns.cycles_join = cyc[2];
@@ -682,6 +1010,10 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, int order, msa_o
         ctx->nj_last = ns;
     }
     if(err == 2) return set_error(ctx, MSA_ERR_UNDEFINED, "no joinable pair: every Q value is NaN");
+    if(err == 4) return set_error(ctx, MSA_ERR_CUDA, "neighbor-joining chose a pair outside the matrix");
+    if(err == 3)
+        return set_error(ctx, MSA_ERR_DEVICE_TIMEOUT,
+                         "a wait between the neighbor-joining clusters ran out; the tree was not built");
 
     // star tree (src/phylogeny/njoining/star.cuh:61-72). The kernel records
     // logical indices; the OTU in each slot follows the same moves (slot of x

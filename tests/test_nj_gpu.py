@@ -130,3 +130,55 @@ def test_c4_tree_matches_reference(gpu):
 def test_small_inputs():
     assert len(phylogeny.run_triangle(np.zeros(0, np.float32), 1)) == 0
     assert len(phylogeny.run_triangle(np.zeros(0, np.float32), 0)) == 0
+
+
+def _set_clusters(clusters, min_count=0, wait_us=0, stall=0):
+    from msa_b200 import runtime
+    _lib.check(_lib.lib().msa_nj_set_clusters(runtime.context(0).handle, clusters, min_count, wait_us, stall))
+
+
+def _last_stats():
+    import ctypes
+    from msa_b200 import runtime
+    ns = _lib.MsaNjStats()
+    _lib.check(_lib.lib().msa_nj_last_stats(runtime.context(0).handle, ctypes.byref(ns)))
+    return ns
+
+
+@pytest.mark.parametrize("order", [_lib.MSA_NJ_SYMMETRIC, _lib.MSA_NJ_LINEAR])
+@pytest.mark.parametrize("n,kind", [(9, "ties"), (60, "ties"), (200, "ties"), (700, "wide"), (1500, "fraction")])
+def test_helper_clusters_give_the_same_tree(gpu, order, n, kind):
+    """Helper clusters scanning beside the joining one (from 8 OTUs on, so
+    small matrices use them too) change nothing in the tree."""
+    tri = _matrix(n, kind, np.random.default_rng(3000 + n))
+    want = O.oracle_nj(tri, n, "linear" if order == _lib.MSA_NJ_LINEAR else "symmetric")
+    try:
+        for clusters in (1, 2, 4):
+            _set_clusters(clusters, 8)
+            assert_same_tree(phylogeny.run_triangle(tri, n, order=order), want)
+            if clusters > 1 and n > 9:
+                assert _last_stats().helper_clusters >= 1
+    finally:
+        _set_clusters(0)
+
+
+def test_wait_between_clusters_runs_out_and_the_context_stays_usable(gpu):
+    """With the joining cluster's hand-over withheld (test hook), the helpers'
+    wait for it and then the joining cluster's wait for their candidates run
+    out: the call fails with MSA_ERR_DEVICE_TIMEOUT, and the next call on the
+    same context builds the right tree."""
+    n = 300
+    tri = _matrix(n, "wide", np.random.default_rng(77))
+    raised = None
+    try:
+        _set_clusters(2, 8, 20000, 1)
+        try:
+            phylogeny.run_triangle(tri, n)
+        except _lib.MsaError as e:
+            raised = e
+        if _last_stats().helper_clusters == 0:
+            pytest.skip("no second cluster could be resident beside the first")
+        assert raised is not None and raised.status == _lib.MSA_ERR_DEVICE_TIMEOUT
+    finally:
+        _set_clusters(0)
+    assert_same_tree(phylogeny.run_triangle(tri, n), O.oracle_nj(tri, n))
