@@ -77,6 +77,33 @@ __device__ __forceinline__ uint32_t order_key(float q)
     return (b & 0x80000000u) ? ~b : (b | 0x80000000u);
 }
 
+// Two float lanes in one 64-bit register and the packed float operations of
+// sm_100 on them: each lane is rounded to nearest as the scalar operation
+// (no flush to zero), so `sub2(sub2(mul2(a, b), c), d)` gives per lane the
+// bits of __fsub_rn(__fsub_rn(__fmul_rn(a, b), c), d) with half the issues.
+__device__ __forceinline__ unsigned long long f2(float a, float b)
+{
+    unsigned long long r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void f2_split(unsigned long long v, float &a, float &b)
+{
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long mul2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigned long long b)
+{
+    unsigned long long r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
 // Larger Q wins; on equal Q the smaller row-major index (earlier in the
 // reference's scan) wins. 0 means "no candidate".
 __device__ __forceinline__ unsigned long long pack(uint32_t key, uint32_t lin)
@@ -169,9 +196,9 @@ __device__ __forceinline__ uint32_t wait_flag(const uint32_t *flag, uint32_t wan
 // fall in different CTAs and the partial block spreads over all of them
 // (with rows ascending and gw = s * 32 + warp, the longest leftover rows all
 // fell to the first CTAs). The CTA's copy of
-// S holds +inf in the dropped slots (< t) and in `moved`'s slot, so those
-// columns give Q = -inf or NaN and never win; the new node's column and the
-// cells past a row's end are masked. Each lane keeps, per row, the largest
+// S holds +inf in the dropped slots (< t), in `moved`'s slot and in the new
+// node's (`pend`), so those columns give Q = -inf or NaN and never win; only
+// the cells past a row's end are masked. Each lane keeps, per row, the largest
 // chunk maximum and the first chunk reaching it, and its best over rows by
 // (Q, row, chunk), which orders like the row-major index; the element inside
 // the winning chunk is resolved once, after the scan. `moved`'s column of
@@ -196,22 +223,22 @@ __device__ __forceinline__ void scan_rows(const ScanView &v, uint32_t s, uint32_
             best_xy = (i << 16) | j;
         }
     };
-    const uint32_t skip1 = v.pend == kNone ? kNone : v.t + v.pend;
     const uint32_t base4 = v.t & ~3u;
     const float s_moved = v.s_moved;
+    const unsigned long long cm2x2 = f2(v.cm2, v.cm2);
     auto row_of = [&](uint32_t i) { return v.D + (size_t) (i == v.moved ? v.mslot : v.t + i) * v.P + base4; };
-    auto chunk_q = [&](const float4 &d, uint32_t col, uint32_t hi, float si, float &q0, float &q1, float &q2,
-                       float &q3) {
+    // Q = (c-2) * D - S_i - S_j for the four cells of a chunk, two per packed
+    // operation; cells at or past the row's end (column hi) get -inf.
+    auto chunk_q = [&](const float4 &d, uint32_t col, uint32_t hi, unsigned long long si2, float &q0, float &q1,
+                       float &q2, float &q3) {
         const float4 s = *reinterpret_cast<const float4 *>(v.S + col);
-        q0 = __fsub_rn(__fsub_rn(__fmul_rn(v.cm2, d.x), si), s.x);
-        q1 = __fsub_rn(__fsub_rn(__fmul_rn(v.cm2, d.y), si), s.y);
-        q2 = __fsub_rn(__fsub_rn(__fmul_rn(v.cm2, d.z), si), s.z);
-        q3 = __fsub_rn(__fsub_rn(__fmul_rn(v.cm2, d.w), si), s.w);
-        if(col + 4 > hi || skip1 - col < 4u) {
-            if(col >= hi || col == skip1) q0 = -INFINITY;
-            if(col + 1 >= hi || col + 1 == skip1) q1 = -INFINITY;
-            if(col + 2 >= hi || col + 2 == skip1) q2 = -INFINITY;
-            if(col + 3 >= hi || col + 3 == skip1) q3 = -INFINITY;
+        f2_split(sub2(sub2(mul2(cm2x2, f2(d.x, d.y)), si2), f2(s.x, s.y)), q0, q1);
+        f2_split(sub2(sub2(mul2(cm2x2, f2(d.z, d.w)), si2), f2(s.z, s.w)), q2, q3);
+        if(col + 4 > hi) {
+            if(col >= hi) q0 = -INFINITY;
+            if(col + 1 >= hi) q1 = -INFINITY;
+            if(col + 2 >= hi) q2 = -INFINITY;
+            if(col + 3 >= hi) q3 = -INFINITY;
         }
     };
     // The row of the warp's place p (p = 0 is row c-1), or 0 past the end.
@@ -240,6 +267,7 @@ __device__ __forceinline__ void scan_rows(const ScanView &v, uint32_t s, uint32_
             const uint32_t hi = v.t + i;
             const float *row = row_of(i);
             const float si = i == v.moved ? s_moved : v.S[v.t + i];
+            const unsigned long long si2 = f2(si, si);
             const uint32_t nch = (hi - base4 + 3) >> 2;
             float bq = -INFINITY;
             uint32_t bg = 0;
@@ -253,7 +281,7 @@ __device__ __forceinline__ void scan_rows(const ScanView &v, uint32_t s, uint32_
                     const uint32_t g = g0 + 32 * u;
                     if(g < nch) {
                         float q0, q1, q2, q3;
-                        chunk_q(d[u], base4 + 4 * g, hi, si, q0, q1, q2, q3);
+                        chunk_q(d[u], base4 + 4 * g, hi, si2, q0, q1, q2, q3);
                         const float m = fmaxf(fmaxf(q0, q1), fmaxf(q2, q3));
                         if(m > bq) {
                             bq = m;
@@ -284,7 +312,8 @@ __device__ __forceinline__ void scan_rows(const ScanView &v, uint32_t s, uint32_
         const uint32_t i = tail >> 14, g = tail & 0x3fffu, col = base4 + 4 * g;
         const float si = i == v.moved ? s_moved : v.S[v.t + i];
         float q[4];
-        chunk_q(__ldcg(reinterpret_cast<const float4 *>(row_of(i) + 4 * g)), col, v.t + i, si, q[0], q[1], q[2], q[3]);
+        chunk_q(__ldcg(reinterpret_cast<const float4 *>(row_of(i) + 4 * g)), col, v.t + i, f2(si, si), q[0], q[1],
+                q[2], q[3]);
         const uint32_t key = (uint32_t) (lbest >> 32);
         int k = 3;
         if(order_key(q[2]) == key) k = 2;   // keep the first element equal to the maximum
@@ -366,12 +395,14 @@ __device__ void nj_helper(const State &st, float *S, uint32_t hidx, uint32_t sid
         const bool mv = Linear ? x != c - 1 : y != 0;
         if(tid == 0) {
             // As the scanning CTAs of cluster 0 (update_cache): the moved
-            // data's row sum aside, +inf in its slot and in a dropped slot.
+            // data's row sum aside, +inf in its slot, in a dropped slot and
+            // in the new node's (published before its fold).
             if(mv) {
                 h_moved = S[t + y];
                 S[t + y] = INFINITY;
             }
             if(!Linear) S[t] = INFINITY;
+            S[Linear && !mv ? y : t + x] = INFINITY;   // the new node's slot
         }
         if(Linear) {
             pend = mv ? x : y;
@@ -411,6 +442,9 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
     __shared__ unsigned long long cyc[kCycleSlots];
     // Row sum of `moved` while this CTA's S holds +inf in its slot (CTAs 0..F-1).
     __shared__ float s_moved_sh;
+    // Row sum of the new node `pend`, written here by CTA F after its fold,
+    // while this CTA's S holds +inf in its slot (CTAs 0..F-1).
+    __shared__ float s_pend_sh;
 
     const unsigned K = cluster.num_blocks();
     const unsigned rank = cluster.block_rank();
@@ -432,6 +466,7 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
     if(tid < kCycleSlots) cyc[tid] = 0;
     if(tid == 0) {
         s_moved_sh = 0.0f;
+        s_pend_sh = 0.0f;
         hoff = 0;
     }
     unsigned long long t_last = clock64();
@@ -475,9 +510,9 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
         if(!folder) {
             // Rows i = 1..c-1 of the logical lower triangle; warp w takes rows
             // w and 2W-1-w of every 2W, so long and short rows pair up. This
-            // CTA's copy of S holds +inf in the dropped slots (< t) and in
-            // `moved`'s slot, so those columns give Q = -inf or NaN and never
-            // win; the new node's column and the cells past a row's end are
+            // CTA's copy of S holds +inf in the dropped slots (< t), in
+            // `moved`'s slot and in the new node's, so those columns give
+            // Q = -inf or NaN and never win; the cells past a row's end are
             // masked. Each lane keeps, per row, the largest chunk maximum and
             // the first chunk reaching it, and its best over rows by (Q, row,
             // chunk), which orders like the row-major index; the element
@@ -601,10 +636,13 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
         const uint32_t wi = wlo + tid;
         const float v0 = (wi < whi && mv) ? __ldcg(r0 + wi) : 0.0f;
 
-        // The scanning CTAs hold +inf in `moved`'s slot of S during a scan;
-        // its row sum is s_moved_sh, which the join reads in its place.
+        // The scanning CTAs hold +inf in the slots of `moved` and `pend` in S
+        // during a scan; their row sums are s_moved_sh and s_pend_sh, which
+        // the join reads in their place.
         const uint32_t mvd = folder ? kNone : moved;
-        const float s_moved = s_moved_sh;
+        const uint32_t pnd = folder ? kNone : pend;
+        const float s_moved = s_moved_sh, s_pend = s_pend_sh;
+        auto s_of = [&](uint32_t i) { return i == mvd ? s_moved : i == pnd ? s_pend : S[t + i]; };
 
         // join_pair (sequential.cpp:247-267). D[i][x] and D[i][y] are read as
         // row x and row y (the matrix is symmetric bit for bit); i = x and
@@ -622,9 +660,9 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             U[i] = u;
             ND[i] = nd;
             exact = exact && ((double) nd == u);
-            const float s_old = i == mvd ? s_moved : S[t + i];
+            const float s_old = s_of(i);
             if(rank == 0 && i == y) {
-                const float sx = x == mvd ? s_moved : S[t + x];
+                const float sx = s_of(x);
                 const float pairsum = __fsub_rn(sx, s_old);
                 const float den = (float) (2u * (c - 2));
                 const float q = __fdiv_rn(pairsum, den);
@@ -650,10 +688,14 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
         exact = __syncthreads_and(exact);
         // update_cache (sequential.cpp:189-224): logical `src` takes y's
         // place. The scanning CTAs keep that row sum aside and put +inf in its
-        // slot, and in logical 0's (symmetric: dropped next), for the next
-        // scan. The linear order's dropped slot c-1 lies past every row the
-        // next scan reads. When the new node takes y's place, its folded sum
-        // arrives there after barrier B.
+        // slot, in logical 0's (symmetric: dropped next) and in the new
+        // node's slot `nslot` (x's, or y's when the new node takes y's place),
+        // for the next scan. The linear order's dropped slot c-1 lies past
+        // every row the next scan reads. The new node's folded sum arrives
+        // after barrier B: in CTA F's S, and in s_pend_sh elsewhere; the next
+        // join writes every slot but x's from the sums it read, so a +inf
+        // slot ends up with its sum unless it is masked again.
+        const uint32_t nslot = Linear && !mv ? y : t + x;
         if(tid == 0) {
             if(folder) {
                 if(mv) S[t + y] = S[t + src];
@@ -663,6 +705,7 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
                     S[t + y] = INFINITY;
                 }
                 if(!Linear) S[t] = INFINITY;
+                S[nslot] = INFINITY;
             }
         }
         // The row sums after this join and the joined pair, for the helper
@@ -710,8 +753,10 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             }
             cluster_wait();
             if(warp == 0) {
-                const uint32_t nslot = Linear && !mv ? y : t + x;
-                if((unsigned) lane < K) cluster.map_shared_rank(S, (unsigned) lane)[nslot] = ns;
+                if((unsigned) lane == F)
+                    S[nslot] = ns;
+                else if((unsigned) lane < K)
+                    *cluster.map_shared_rank(&s_pend_sh, (unsigned) lane) = ns;
             }
             __syncthreads();   // the folded row sum is in this CTA's S
             if(timer) t_last = clock64();
