@@ -104,12 +104,15 @@ __device__ __forceinline__ unsigned long long sub2(unsigned long long a, unsigne
     return r;
 }
 
-// Larger Q wins; on equal Q the smaller row-major index (earlier in the
-// reference's scan) wins. 0 means "no candidate".
-__device__ __forceinline__ unsigned long long pack(uint32_t key, uint32_t lin)
+// A candidate pair (i, j), j < i, as one 64-bit key: larger Q wins; on equal
+// Q the pair earlier in the reference's row-major scan of the lower triangle
+// (smaller i, then smaller j) wins, which is the order of i << 16 | j (i, j <
+// 2^16). 0 means "no candidate"; the low word names the pair.
+__device__ __forceinline__ unsigned long long pack(uint32_t key, uint32_t i, uint32_t j)
 {
-    return key ? (((unsigned long long) key << 32) | (0xffffffffu - lin)) : 0ull;
+    return key ? (((unsigned long long) key << 32) | (0xffffffffu - ((i << 16) | j))) : 0ull;
 }
+__device__ __forceinline__ uint32_t pair_of(unsigned long long v) { return 0xffffffffu - (uint32_t) v; }
 
 __device__ __forceinline__ unsigned long long umax64(unsigned long long a, unsigned long long b) { return a > b ? a : b; }
 
@@ -139,7 +142,7 @@ struct State {
     float *s_pub;              // [2][P] row sums published by the folding CTA after a join
     uint32_t *pub_xy;          // [2] the join (x << 16 | y) they follow
     uint32_t *pub_seq;         // join number + 1 of the last publication; kStop ends the helpers
-    unsigned long long *cand;  // [2][helper_ctas][2] each helper CTA's candidate (key, x << 16 | y)
+    unsigned long long *cand;  // [2][helper_ctas] each helper CTA's candidate key
     uint32_t *cand_seq;        // [helper_ctas] join number + 1 of its last candidate
     unsigned long long wait_ns;   // limit of every wait between clusters
     int stall_publication;     // test hook: the folding CTA never publishes
@@ -205,7 +208,7 @@ __device__ __forceinline__ uint32_t wait_flag(const uint32_t *flag, uint32_t wan
 // later rows is read from where its data still is (slot mslot): lane r loads
 // it for the warp's r-th row before the row loop and offers it after, so the
 // load waits in the shadow of the scan. The lane's best candidate goes into
-// (best, best_xy).
+// `best`.
 struct ScanView {
     const float *D;   // slot t + k holds logical k; row pitch P
     const float *S;   // this CTA's row sums by slot
@@ -214,15 +217,9 @@ struct ScanView {
 };
 
 __device__ __forceinline__ void scan_rows(const ScanView &v, uint32_t s, uint32_t ns, int warp, int lane,
-                                          unsigned long long &best, uint32_t &best_xy)
+                                          unsigned long long &best)
 {
     const uint32_t W = ns * kWarps, gw = (uint32_t) warp * ns + s;
-    auto offer = [&](unsigned long long q, uint32_t i, uint32_t j) {
-        if(q > best) {
-            best = q;
-            best_xy = (i << 16) | j;
-        }
-    };
     const uint32_t base4 = v.t & ~3u;
     const float s_moved = v.s_moved;
     const unsigned long long cm2x2 = f2(v.cm2, v.cm2);
@@ -299,7 +296,7 @@ __device__ __forceinline__ void scan_rows(const ScanView &v, uint32_t s, uint32_
         for(uint32_t r = (uint32_t) lane;;) {
             if(mi) {
                 const float q = __fsub_rn(__fsub_rn(__fmul_rn(v.cm2, mq), v.S[v.t + mi]), s_moved);
-                offer(pack(order_key(q), mi * (mi - 1) / 2 + v.moved), mi, v.moved);
+                best = umax64(best, pack(order_key(q), mi, v.moved));
             }
             r += 32;
             if(r >= rows) break;
@@ -320,7 +317,7 @@ __device__ __forceinline__ void scan_rows(const ScanView &v, uint32_t s, uint32_
         if(order_key(q[1]) == key) k = 1;
         if(order_key(q[0]) == key) k = 0;
         const uint32_t j = col + k - v.t;
-        offer(pack(key, i * (i - 1) / 2 + j), i, j);
+        best = umax64(best, pack(key, i, j));
     }
 }
 
@@ -337,7 +334,6 @@ template <bool Linear>
 __device__ void nj_helper(const State &st, float *S, uint32_t hidx, uint32_t sidx, uint32_t nscan)
 {
     __shared__ unsigned long long hbest[kWarps];
-    __shared__ uint32_t hxy[kWarps];
     __shared__ float h_moved;
     __shared__ int h_stop;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -351,12 +347,10 @@ __device__ void nj_helper(const State &st, float *S, uint32_t hidx, uint32_t sid
     uint32_t c = n, t = 0, step = 0, pend = kNone, moved = kNone, mslot = 0;
     while(c > 1 && c > st.helper_c) {
         unsigned long long best = 0;
-        uint32_t best_xy = 0;
         scan_rows(ScanView{st.D, S, P, t, c, pend, moved, mslot, (float) (c - 2), h_moved}, sidx, nscan, warp, lane,
-                  best, best_xy);
+                  best);
         {
             const unsigned long long wm = warp_max(best);
-            if(best == wm && wm != 0ull) hxy[warp] = best_xy;
             if(lane == 0) hbest[warp] = wm;
         }
         __syncthreads();
@@ -364,11 +358,8 @@ __device__ void nj_helper(const State &st, float *S, uint32_t hidx, uint32_t sid
         if(warp == 0) {
             const unsigned long long v = lane < kWarps ? hbest[lane] : 0ull;
             const unsigned long long m = warp_max(v);
-            const uint32_t holder = __ffs(__ballot_sync(kFull, v == m)) - 1;
             if(lane == 0) {
-                unsigned long long *slot = st.cand + ((size_t) buf * st.helper_ctas + hidx) * 2;
-                slot[0] = m;
-                slot[1] = m ? hxy[holder] : 0u;
+                st.cand[(size_t) buf * st.helper_ctas + hidx] = m;
                 st_release(st.cand_seq + hidx, step + 1);
             }
         }
@@ -433,10 +424,9 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
     float *S = reinterpret_cast<float *>(smem_raw);
     float *ND = S + P;
     double *U = reinterpret_cast<double *>(smem_raw + (size_t) 8 * P);
-    __shared__ unsigned long long parts[kMaxCluster];   // each CTA's candidate
-    __shared__ uint32_t part_xy[kMaxCluster];           // and its (x << 16 | y)
+    // Each CTA's best key, written into every CTA before barrier A.
+    __shared__ unsigned long long parts[kMaxCluster];
     __shared__ unsigned long long wbest[kWarps];
-    __shared__ uint32_t wxy[kWarps];
     // Phase cycle counters live in shared memory, leaving registers to the
     // scan's loads in flight.
     __shared__ unsigned long long cyc[kCycleSlots];
@@ -498,27 +488,14 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
         // The helper clusters scan with cluster 0 for this join.
         const bool helped = kHelp && st.helper_ctas != 0u && !hoff && c > st.helper_c;
         unsigned long long best = 0;
-        uint32_t best_xy = 0;
-        auto offer = [&](unsigned long long v, uint32_t i, uint32_t j) {
-            if(v > best) {
-                best = v;
-                best_xy = (i << 16) | j;
-            }
-        };
 
         // ---- scan
         if(!folder) {
-            // Rows i = 1..c-1 of the logical lower triangle; warp w takes rows
-            // w and 2W-1-w of every 2W, so long and short rows pair up. This
-            // CTA's copy of S holds +inf in the dropped slots (< t), in
-            // `moved`'s slot and in the new node's, so those columns give
-            // Q = -inf or NaN and never win; the cells past a row's end are
-            // masked. Each lane keeps, per row, the largest chunk maximum and
-            // the first chunk reaching it, and its best over rows by (Q, row,
-            // chunk), which orders like the row-major index; the element
-            // inside the winning chunk is resolved once, after the scan.
+            // This CTA's share of the rows of the logical lower triangle
+            // (scan_rows), with +inf in S masking the dropped slots and those
+            // of `moved` and the new node.
             scan_rows(ScanView{D, S, P, t, c, pend, moved, mslot, cm2, s_moved_sh}, rank,
-                      F + (helped ? st.helper_ctas : 0u), warp, lane, best, best_xy);
+                      F + (helped ? st.helper_ctas : 0u), warp, lane, best);
         } else if(pend != kNone) {
             // The new node's row and column, from the distances the last join
             // computed (ND, indexed by that join's logical order: logical j
@@ -533,53 +510,37 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
                 const float sj = S[t + j];
                 if(j < x) {
                     const float q = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d), sx), sj);
-                    offer(pack(order_key(q), x * (x - 1) / 2 + j), x, j);
+                    best = umax64(best, pack(order_key(q), x, j));
                 } else {
                     const float q = __fsub_rn(__fsub_rn(__fmul_rn(cm2, d), sj), sx);
-                    offer(pack(order_key(q), j * (j - 1) / 2 + x), j, x);
+                    best = umax64(best, pack(order_key(q), j, x));
                 }
             }
         }
-        // Candidates are unique (distinct indices), so the holder of the
-        // maximum also names its (x, y).
+        // Keys are unique (distinct pairs) and name their pair, so the
+        // maximum over all CTAs is the join.
         {
             const unsigned long long wm = warp_max(best);
-            if(best == wm && wm != 0ull) wxy[warp] = best_xy;
             if(lane == 0) wbest[warp] = wm;
         }
         __syncthreads();
         if(warp == 0) {
             const unsigned long long v = lane < kWarps ? wbest[lane] : 0ull;
             unsigned long long m = warp_max(v);
-            const uint32_t holder = __ffs(__ballot_sync(kFull, v == m)) - 1;
-            uint32_t xy = m ? wxy[holder] : 0u;
             int off = 0;
             if(kHelp && rank == 0 && helped) {
                 // The helper CTAs' candidates for this join, each lane waiting
                 // for its share of them; merged into this CTA's part.
                 const uint32_t buf = step & 1u;
                 unsigned long long hb = 0;
-                uint32_t hxyv = 0;
                 bool ok = true;
                 for(uint32_t h = lane; h < st.helper_ctas; h += 32) {
-                    if(ok && wait_flag(st.cand_seq + h, step + 1, st.wait_ns) != 0u) {
-                        const unsigned long long *slot = st.cand + ((size_t) buf * st.helper_ctas + h) * 2;
-                        const unsigned long long key = __ldcg(slot);
-                        if(key > hb) {
-                            hb = key;
-                            hxyv = (uint32_t) __ldcg(slot + 1);
-                        }
-                    } else {
+                    if(ok && wait_flag(st.cand_seq + h, step + 1, st.wait_ns) != 0u)
+                        hb = umax64(hb, __ldcg(st.cand + (size_t) buf * st.helper_ctas + h));
+                    else
                         ok = false;
-                    }
                 }
-                const unsigned long long hm = warp_max(hb);
-                const uint32_t hh = __ffs(__ballot_sync(kFull, hb == hm)) - 1;
-                const uint32_t hmxy = __shfl_sync(kFull, hxyv, hh);
-                if(hm > m) {
-                    m = hm;
-                    xy = hmxy;
-                }
+                m = umax64(m, warp_max(hb));
                 if(!__all_sync(kFull, ok)) {
                     off = 1;
                     if(lane == 0) atomicExch(st.err, 3);
@@ -587,7 +548,6 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             }
             if((unsigned) lane < K) {
                 cluster.map_shared_rank(parts, (unsigned) lane)[rank] = m;
-                cluster.map_shared_rank(part_xy, (unsigned) lane)[rank] = xy;
                 if(off) cluster.map_shared_rank(&hoff, (unsigned) lane)[0] = 1;
             }
         }
@@ -597,18 +557,13 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
         if(timer) mark(rank == 0 ? 1 : 7);
 
         // ---- join
-        unsigned long long win = 0;
-        unsigned wr = 0;
-        for(unsigned r = 0; r < K; ++r)
-            if(parts[r] > win) {
-                win = parts[r];
-                wr = r;
-            }
+        // Every warp reduces the K parts itself (lane r reads part r).
+        const unsigned long long win = warp_max((unsigned) lane < K ? parts[lane] : 0ull);
         if(win == 0ull) {   // no selectable Q (all NaN): the reference would index an undefined pair
             failed = true;
             break;
         }
-        const uint32_t x = part_xy[wr] >> 16, y = part_xy[wr] & 0xffffu;
+        const uint32_t x = pair_of(win) >> 16, y = pair_of(win) & 0xffffu;
         if(x >= c || y >= x) {   // never a pair of this join: report it, touch nothing
             bad = true;
             break;
@@ -622,119 +577,56 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
         const float *rx = D + (size_t) (t + x) * P + t;
         const float *ry = D + (size_t) (t + y) * P + t;
         const float *r0 = D + (size_t) (t + src) * P + t;
-        // Every load this thread's first two join elements need is issued
-        // here, before the bookkeeping below: one L2 round trip for all of
-        // them (c <= 2048); later elements are loaded two iterations ahead.
         const float dxy = __ldcg(rx + y);
-        float a0 = (uint32_t) tid < c ? __ldcg(rx + tid) : 0.0f, b0 = (uint32_t) tid < c ? __ldcg(ry + tid) : 0.0f;
-        const uint32_t i1 = tid + kThreads;
-        float a1 = i1 < c ? __ldcg(rx + i1) : 0.0f, b1 = i1 < c ? __ldcg(ry + i1) : 0.0f;
-        // This thread's first element of the write slice (CTAs 0..F-1):
-        // the moved row's entry, loaded now so the writes wait for no load.
-        const uint32_t wlo = folder ? 0 : (uint32_t) ((uint64_t) c * rank / F);
-        const uint32_t whi = folder ? 0 : (uint32_t) ((uint64_t) c * (rank + 1) / F);
-        const uint32_t wi = wlo + tid;
-        const float v0 = (wi < whi && mv) ? __ldcg(r0 + wi) : 0.0f;
-
-        // The scanning CTAs hold +inf in the slots of `moved` and `pend` in S
-        // during a scan; their row sums are s_moved_sh and s_pend_sh, which
-        // the join reads in their place.
-        const uint32_t mvd = folder ? kNone : moved;
-        const uint32_t pnd = folder ? kNone : pend;
-        const float s_moved = s_moved_sh, s_pend = s_pend_sh;
-        auto s_of = [&](uint32_t i) { return i == mvd ? s_moved : i == pnd ? s_pend : S[t + i]; };
-
-        // join_pair (sequential.cpp:247-267). D[i][x] and D[i][y] are read as
-        // row x and row y (the matrix is symmetric bit for bit); i = x and
-        // i = y read the diagonal and D[x][y], as the reference does. The
-        // thread of element y in CTA 0 also computes raise_candidate
-        // (sequential.cpp:142-152) from the row sums before this join's
-        // update (S[x] is not updated here, S[y] is read before it is).
-        bool exact = true;
-        for(uint32_t i = tid; i < c; i += kThreads) {
-            const uint32_t in = i + 2 * kThreads;
-            const float an = in < c ? __ldcg(rx + in) : 0.0f, bn = in < c ? __ldcg(ry + in) : 0.0f;
-            const float prev = __fadd_rn(a0, b0);
-            const double u = __dmul_rn((double) __fsub_rn(prev, dxy), 0.5);
-            const float nd = __double2float_rn(u);
-            U[i] = u;
-            ND[i] = nd;
-            exact = exact && ((double) nd == u);
-            const float s_old = s_of(i);
-            if(rank == 0 && i == y) {
-                const float sx = s_of(x);
-                const float pairsum = __fsub_rn(sx, s_old);
-                const float den = (float) (2u * (c - 2));
-                const float q = __fdiv_rn(pairsum, den);
-                float dx = __double2float_rn(__dadd_rn(__dmul_rn(0.5, (double) dxy), (double) q));
-                float dy = __fsub_rn(dxy, dx);
-                // The last join divides by 2(c-2) = 0; for 0/0 the reference's
-                // x86 SSE arithmetic yields the default NaN 0xFFC00000 and
-                // propagates it into dx and dy, where the GPU would give its
-                // canonical 0x7FFFFFFF.
-                if(dx != dx) dx = __uint_as_float(0xFFC00000u);
-                if(dy != dy) dy = __uint_as_float(0xFFC00000u);
-                st.rec_x[step] = x;
-                st.rec_y[step] = y;
-                st.rec_dx[step] = dx;
-                st.rec_dy[step] = dy;
-            }
-            if(i != x) S[t + i] = __double2float_rn(__dadd_rn((double) s_old, __dsub_rn(u, (double) prev)));
-            a0 = a1;
-            b0 = b1;
-            a1 = an;
-            b1 = bn;
-        }
-        exact = __syncthreads_and(exact);
-        // update_cache (sequential.cpp:189-224): logical `src` takes y's
-        // place. The scanning CTAs keep that row sum aside and put +inf in its
-        // slot, in logical 0's (symmetric: dropped next) and in the new
-        // node's slot `nslot` (x's, or y's when the new node takes y's place),
-        // for the next scan. The linear order's dropped slot c-1 lies past
-        // every row the next scan reads. The new node's folded sum arrives
-        // after barrier B: in CTA F's S, and in s_pend_sh elsewhere; the next
-        // join writes every slot but x's from the sums it read, so a +inf
-        // slot ends up with its sum unless it is masked again.
         const uint32_t nslot = Linear && !mv ? y : t + x;
-        if(tid == 0) {
-            if(folder) {
-                if(mv) S[t + y] = S[t + src];
-            } else {
-                if(mv) {
-                    s_moved_sh = S[t + src];
-                    S[t + y] = INFINITY;
-                }
-                if(!Linear) S[t] = INFINITY;
-                S[nslot] = INFINITY;
-            }
-        }
-        // The row sums after this join and the joined pair, for the helper
-        // clusters' next scan (the folding CTA's copy has no +inf masks).
-        if(kHelp && folder && st.helper_ctas != 0u && !hoff && c - 1 > st.helper_c) {
-            __syncthreads();   // update_cache above
-            const uint32_t buf = step & 1u;
-            float *pub = st.s_pub + (size_t) buf * P;
-            for(uint32_t k = t + tid; k < t + c; k += kThreads) __stcg(pub + k, S[k]);
-            if(tid == 0) st.pub_xy[buf] = (x << 16) | y;
-            __syncthreads();
-            if(tid == 0 && !st.stall_publication) {
-                __threadfence();
-                st_release(st.pub_seq, step + 1);
-            }
-        }
-        if(timer && rank == 0) mark(2);
-        cluster_arrive();   // B: every read of rows x, y and the moved row is done
+        // Row sums of the new node and of the moved data, held aside while a
+        // scanning CTA's S has +inf in their slots.
+        const float s_moved = s_moved_sh, s_pend = s_pend_sh;
 
         if(folder) {
+            // CTA F computes the whole join for its own S, ND and U (the fold
+            // needs all of them), but only its reads of rows x and y come
+            // before barrier B (the writes after B change those rows): it
+            // keeps D[x][i] + D[y][i] in ND, arrives, and finishes after.
+            for(uint32_t i = tid; i < c; i += kThreads) ND[i] = __fadd_rn(__ldcg(rx + i), __ldcg(ry + i));
+            cluster_arrive();   // B
+            // join_pair (sequential.cpp:247-267); i = x and i = y read the
+            // diagonal and D[x][y], as the reference does. S has no masks here.
+            bool exact = true;
+            for(uint32_t i = tid; i < c; i += kThreads) {
+                const float prev = ND[i];
+                const double u = __dmul_rn((double) __fsub_rn(prev, dxy), 0.5);
+                const float nd = __double2float_rn(u);
+                U[i] = u;
+                ND[i] = nd;
+                exact = exact && ((double) nd == u);
+                if(i != x) S[t + i] = __double2float_rn(__dadd_rn((double) S[t + i], __dsub_rn(u, (double) prev)));
+            }
+            exact = __syncthreads_and(exact);
+            // update_cache (sequential.cpp:189-224): logical `src` takes y's place.
+            if(tid == 0 && mv) S[t + y] = S[t + src];
+            // The row sums after this join and the joined pair, for the helper
+            // clusters' next scan (this CTA's copy has no +inf masks).
+            if(kHelp && st.helper_ctas != 0u && !hoff && c - 1 > st.helper_c) {
+                __syncthreads();   // update_cache above
+                const uint32_t buf = step & 1u;
+                float *pub = st.s_pub + (size_t) buf * P;
+                for(uint32_t k = t + tid; k < t + c; k += kThreads) __stcg(pub + k, S[k]);
+                if(tid == 0) st.pub_xy[buf] = (x << 16) | y;
+                __syncthreads();
+                if(tid == 0 && !st.stall_publication) {
+                    __threadfence();
+                    st_release(st.pub_seq, step + 1);
+                }
+            }
             // Serial fold of the new row sum, i ascending. When every update is
             // a float value, the double add rounded to float equals a float add
             // (double has >= 2*24+2 significand bits), so the short float chain
             // is used; otherwise the literal double one. Warp 0 runs it (every
             // lane the same chain, reading ND by broadcast 16-byte loads that
-            // do not depend on the chain) while barrier B completes: the fold
-            // reads only this CTA's ND and U, written before this thread's
-            // __syncthreads_and above. Its result goes into every CTA's S only
-            // after B, when no CTA still updates its row sums for this join.
+            // do not depend on the chain); ND and U were written before the
+            // __syncthreads_and above. The sum goes to the other CTAs after B,
+            // when none of them still reads s_pend_sh for this join.
             float ns = 0.0f;
             if(warp == 0) {
                 const unsigned long long f0 = clock64();
@@ -761,16 +653,95 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             __syncthreads();   // the folded row sum is in this CTA's S
             if(timer) t_last = clock64();
         } else {
+            // The scanning CTAs split the join: CTA r < F takes the elements
+            // [c r / F, c (r + 1) / F), the slice it also writes back after B.
+            // The loads of a thread's first element are issued here, and the
+            // moved row's entry too, so the writes wait for no load.
+            const uint32_t jlo = (uint32_t) ((uint64_t) c * rank / F);
+            const uint32_t jhi = (uint32_t) ((uint64_t) c * (rank + 1) / F);
+            const uint32_t ji = jlo + tid;
+            float a0 = ji < jhi ? __ldcg(rx + ji) : 0.0f, b0 = ji < jhi ? __ldcg(ry + ji) : 0.0f;
+            const float v0 = (ji < jhi && mv) ? __ldcg(r0 + ji) : 0.0f;
+            auto s_of = [&](uint32_t i) { return i == moved ? s_moved : i == pend ? s_pend : S[t + i]; };
+
+            // join_pair (sequential.cpp:247-267) on the slice. D[i][x] and
+            // D[i][y] are read as row x and row y (the matrix is symmetric bit
+            // for bit); i = x and i = y read the diagonal and D[x][y], as the
+            // reference does. Each new row sum goes into every scanning CTA's
+            // S; the thread of element y also computes raise_candidate
+            // (sequential.cpp:142-152) from the row sums before this join's
+            // update (S[x] is not updated here, S[y] is read before it is).
+            for(uint32_t i = ji; i < jhi; i += kThreads) {
+                const uint32_t in = i + kThreads;
+                const float an = in < jhi ? __ldcg(rx + in) : 0.0f, bn = in < jhi ? __ldcg(ry + in) : 0.0f;
+                const float prev = __fadd_rn(a0, b0);
+                const double u = __dmul_rn((double) __fsub_rn(prev, dxy), 0.5);
+                ND[i] = __double2float_rn(u);
+                const float s_old = s_of(i);
+                if(i == y) {
+                    const float sx = s_of(x);
+                    const float pairsum = __fsub_rn(sx, s_old);
+                    const float den = (float) (2u * (c - 2));
+                    const float q = __fdiv_rn(pairsum, den);
+                    float dx = __double2float_rn(__dadd_rn(__dmul_rn(0.5, (double) dxy), (double) q));
+                    float dy = __fsub_rn(dxy, dx);
+                    // The last join divides by 2(c-2) = 0; for 0/0 the
+                    // reference's x86 SSE arithmetic yields the default NaN
+                    // 0xFFC00000 and propagates it into dx and dy, where the
+                    // GPU would give its canonical 0x7FFFFFFF.
+                    if(dx != dx) dx = __uint_as_float(0xFFC00000u);
+                    if(dy != dy) dy = __uint_as_float(0xFFC00000u);
+                    st.rec_x[step] = x;
+                    st.rec_y[step] = y;
+                    st.rec_dx[step] = dx;
+                    st.rec_dy[step] = dy;
+                }
+                if(i != x) {
+                    const float sn = __double2float_rn(__dadd_rn((double) s_old, __dsub_rn(u, (double) prev)));
+                    for(unsigned r = 0; r < F; ++r) cluster.map_shared_rank(S, r)[t + i] = sn;
+                }
+                a0 = an;
+                b0 = bn;
+            }
+            if(timer && rank == 0) mark(2);
+            // B: every read of rows x, y and the moved row is done, and every
+            // slice's row sums are in every scanning CTA's S.
+            cluster_arrive();
             cluster_wait();
             if(timer) mark(3);
-            // Row/column x get the new distances; logical 0's row/column move
+            // update_cache (sequential.cpp:189-224): logical `src` takes y's
+            // place. Keep that row sum aside and put +inf in its slot, in
+            // logical 0's (symmetric: dropped next) and in the new node's slot
+            // `nslot` (x's, or y's when the new node takes y's place), for the
+            // next scan. The linear order's dropped slot c-1 lies past every
+            // row the next scan reads. The new node's folded sum arrives in
+            // s_pend_sh; the next join writes every slot but x's from the sums
+            // it read, so a +inf slot ends up with its sum unless it is masked
+            // again.
+            if(tid == 0) {
+                if(mv) {
+                    s_moved_sh = S[t + src];
+                    S[t + y] = INFINITY;
+                }
+                if(!Linear) S[t] = INFINITY;
+                S[nslot] = INFINITY;
+            }
+            // The new distance of logical `src` (for row and column x), from
+            // the scanning CTA whose slice holds it.
+            auto nd_src = [&]() {
+                unsigned r = 0;
+                while(r + 1 < F && (uint64_t) c * (r + 1) / F <= src) ++r;
+                return cluster.map_shared_rank(ND, r)[src];
+            };
+            // Row/column x get the new distances (this CTA's slice of them is
+            // in its ND, all of them in CTA F's); logical 0's row/column move
             // into y.
             float *wx = D + (size_t) (t + x) * P + t;
             float *wy = D + (size_t) (t + y) * P + t;
             if(Linear) {
                 // Row/column x get the new distances and row/column c-1 move
                 // into y; or, when x is c-1, the new distances go into y.
-                for(uint32_t i = wi; i < whi; i += kThreads) {
+                for(uint32_t i = ji; i < jhi; i += kThreads) {
                     if(mv) {
                         if(i == c - 1) continue;
                         if(i == y) {
@@ -779,14 +750,15 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
                         }
                         if(i == x) {
                             __stcg(wx + x, ND[x]);
-                            __stcg(wx + y, ND[c - 1]);
-                            __stcg(wy + x, ND[c - 1]);
+                            const float nds = nd_src();
+                            __stcg(wx + y, nds);
+                            __stcg(wy + x, nds);
                             continue;
                         }
                         const float nd = ND[i];
                         __stcg(wx + i, nd);
                         __stcg(D + (size_t) i * P + x, nd);
-                        const float v = i == wi ? v0 : __ldcg(r0 + i);
+                        const float v = i == ji ? v0 : __ldcg(r0 + i);
                         __stcg(wy + i, v);
                         __stcg(D + (size_t) i * P + y, v);
                     } else {
@@ -797,7 +769,7 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
                     }
                 }
             } else
-            for(uint32_t i = wi; i < whi; i += kThreads) {
+            for(uint32_t i = ji; i < jhi; i += kThreads) {
                 if(i == 0 || i == y) {
                     if(i == y && y != 0) __stcg(wy + y, __ldcg(r0));   // logical 0's diagonal
                     continue;
@@ -805,8 +777,9 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
                 if(i == x) {
                     __stcg(wx + x, ND[x]);
                     if(y != 0) {
-                        __stcg(wx + y, ND[0]);
-                        __stcg(wy + x, ND[0]);
+                        const float nds = nd_src();
+                        __stcg(wx + y, nds);
+                        __stcg(wy + x, nds);
                     }
                     continue;
                 }
@@ -814,11 +787,12 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
                 __stcg(wx + i, nd);
                 __stcg(D + (size_t) (t + i) * P + t + x, nd);
                 if(y != 0) {
-                    const float v = i == wi ? v0 : __ldcg(r0 + i);
+                    const float v = i == ji ? v0 : __ldcg(r0 + i);
                     __stcg(wy + i, v);
                     __stcg(D + (size_t) (t + i) * P + t + y, v);
                 }
             }
+            __syncthreads();   // the +inf masks above, before the scan
             if(timer) mark(4);
         }
 
@@ -1002,6 +976,10 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, int order, msa_o
     njdev::row_sums_kernel<<<(n + 255) / 256, 256, 0, s>>>(st.D, (float *) (base + oS), n, P);
     MSA_CUDA_TRY(ctx, cudaGetLastError());
     MSA_CUDA_TRY(ctx, cudaMemsetAsync(base + oErr, 0, 64, s));
+    // Joins the kernel never records stay invalid (0xffffffff) and are caught
+    // before the tree is built.
+    MSA_CUDA_TRY(ctx, cudaMemsetAsync(base + oRx, 0xff, (size_t) n * 4, s));
+    MSA_CUDA_TRY(ctx, cudaMemsetAsync(base + oRy, 0xff, (size_t) n * 4, s));
     MSA_CUDA_TRY(ctx, cudaMemsetAsync(base + oCyc, 0, 64, s));
     MSA_CUDA_TRY(ctx, cudaMemsetAsync(sync, 0, 64 + (size_t) njdev::kMaxHelperCtas * 4, s));
     ctx->launches += 2;
@@ -1059,6 +1037,10 @@ int nj_run(msa_ctx *ctx, const void *tri, int kind, uint32_t n, int order, msa_o
     if(err == 3)
         return set_error(ctx, MSA_ERR_DEVICE_TIMEOUT,
                          "a wait between the neighbor-joining clusters ran out; the tree was not built");
+
+    for(uint32_t k = 0; k + 1 < n; ++k)
+        if(rx[k] >= n - k || ry[k] >= rx[k])
+            return set_error(ctx, MSA_ERR_CUDA, "neighbor-joining recorded an invalid join");
 
     // star tree (src/phylogeny/njoining/star.cuh:61-72). The kernel records
     // logical indices; the OTU in each slot follows the same moves (slot of x
