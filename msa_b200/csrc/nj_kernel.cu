@@ -116,11 +116,14 @@ __device__ __forceinline__ uint32_t pair_of(unsigned long long v) { return 0xfff
 
 __device__ __forceinline__ unsigned long long umax64(unsigned long long a, unsigned long long b) { return a > b ? a : b; }
 
+// The warp's maximum of a 64-bit key in two 32-bit warp reductions: the
+// largest high word, then the largest low word among the lanes holding it.
 __device__ __forceinline__ unsigned long long warp_max(unsigned long long v)
 {
-#pragma unroll
-    for(int o = 16; o > 0; o >>= 1) v = umax64(v, __shfl_xor_sync(kFull, v, o));
-    return v;
+    const uint32_t hi = (uint32_t) (v >> 32), lo = (uint32_t) v;
+    const uint32_t mhi = __reduce_max_sync(kFull, hi);
+    const uint32_t mlo = __reduce_max_sync(kFull, hi == mhi ? lo : 0u);
+    return ((unsigned long long) mhi << 32) | mlo;
 }
 
 __device__ __forceinline__ void cluster_arrive() { asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory"); }
@@ -592,6 +595,7 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             cluster_arrive();   // B
             // join_pair (sequential.cpp:247-267); i = x and i = y read the
             // diagonal and D[x][y], as the reference does. S has no masks here.
+            // The thread of element y also computes raise_candidate.
             bool exact = true;
             for(uint32_t i = tid; i < c; i += kThreads) {
                 const float prev = ND[i];
@@ -600,7 +604,28 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
                 U[i] = u;
                 ND[i] = nd;
                 exact = exact && ((double) nd == u);
-                if(i != x) S[t + i] = __double2float_rn(__dadd_rn((double) S[t + i], __dsub_rn(u, (double) prev)));
+                const float s_old = S[t + i];
+                if(i == y) {
+                    // raise_candidate (sequential.cpp:142-152) from the row
+                    // sums before this join's update (S[x] is not updated
+                    // here, S[y] is read before it is).
+                    const float pairsum = __fsub_rn(S[t + x], s_old);
+                    const float den = (float) (2u * (c - 2));
+                    const float q = __fdiv_rn(pairsum, den);
+                    float dx = __double2float_rn(__dadd_rn(__dmul_rn(0.5, (double) dxy), (double) q));
+                    float dy = __fsub_rn(dxy, dx);
+                    // The last join divides by 2(c-2) = 0; for 0/0 the
+                    // reference's x86 SSE arithmetic yields the default NaN
+                    // 0xFFC00000 and propagates it into dx and dy, where the
+                    // GPU would give its canonical 0x7FFFFFFF.
+                    if(dx != dx) dx = __uint_as_float(0xFFC00000u);
+                    if(dy != dy) dy = __uint_as_float(0xFFC00000u);
+                    st.rec_x[step] = x;
+                    st.rec_y[step] = y;
+                    st.rec_dx[step] = dx;
+                    st.rec_dy[step] = dy;
+                }
+                if(i != x) S[t + i] = __double2float_rn(__dadd_rn((double) s_old, __dsub_rn(u, (double) prev)));
             }
             exact = __syncthreads_and(exact);
             // update_cache (sequential.cpp:189-224): logical `src` takes y's place.
@@ -668,9 +693,7 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             // D[i][y] are read as row x and row y (the matrix is symmetric bit
             // for bit); i = x and i = y read the diagonal and D[x][y], as the
             // reference does. Each new row sum goes into every scanning CTA's
-            // S; the thread of element y also computes raise_candidate
-            // (sequential.cpp:142-152) from the row sums before this join's
-            // update (S[x] is not updated here, S[y] is read before it is).
+            // S (CTA F computes raise_candidate in its copy of the join).
             for(uint32_t i = ji; i < jhi; i += kThreads) {
                 const uint32_t in = i + kThreads;
                 const float an = in < jhi ? __ldcg(rx + in) : 0.0f, bn = in < jhi ? __ldcg(ry + in) : 0.0f;
@@ -678,24 +701,6 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
                 const double u = __dmul_rn((double) __fsub_rn(prev, dxy), 0.5);
                 ND[i] = __double2float_rn(u);
                 const float s_old = s_of(i);
-                if(i == y) {
-                    const float sx = s_of(x);
-                    const float pairsum = __fsub_rn(sx, s_old);
-                    const float den = (float) (2u * (c - 2));
-                    const float q = __fdiv_rn(pairsum, den);
-                    float dx = __double2float_rn(__dadd_rn(__dmul_rn(0.5, (double) dxy), (double) q));
-                    float dy = __fsub_rn(dxy, dx);
-                    // The last join divides by 2(c-2) = 0; for 0/0 the
-                    // reference's x86 SSE arithmetic yields the default NaN
-                    // 0xFFC00000 and propagates it into dx and dy, where the
-                    // GPU would give its canonical 0x7FFFFFFF.
-                    if(dx != dx) dx = __uint_as_float(0xFFC00000u);
-                    if(dy != dy) dy = __uint_as_float(0xFFC00000u);
-                    st.rec_x[step] = x;
-                    st.rec_y[step] = y;
-                    st.rec_dx[step] = dx;
-                    st.rec_dy[step] = dy;
-                }
                 if(i != x) {
                     const float sn = __double2float_rn(__dadd_rn((double) s_old, __dsub_rn(u, (double) prev)));
                     for(unsigned r = 0; r < F; ++r) cluster.map_shared_rank(S, r)[t + i] = sn;
@@ -726,67 +731,43 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
                 if(!Linear) S[t] = INFINITY;
                 S[nslot] = INFINITY;
             }
-            // The new distance of logical `src` (for row and column x), from
-            // the scanning CTA whose slice holds it.
-            auto nd_src = [&]() {
-                unsigned r = 0;
-                while(r + 1 < F && (uint64_t) c * (r + 1) / F <= src) ++r;
-                return cluster.map_shared_rank(ND, r)[src];
-            };
-            // Row/column x get the new distances (this CTA's slice of them is
-            // in its ND, all of them in CTA F's); logical 0's row/column move
-            // into y.
+            // The writes of this CTA's slice, after B, overlapping the next
+            // scan (which skips the new node's row, reads the moved data where
+            // it was, and masks columns x and y): row and column x get the new
+            // distances, and logical `src`'s row and column move into y (or,
+            // in the linear order when x is the last, the new distances go
+            // into y). D[x][y] and D[y][x] take src's new distance, from the
+            // scanning CTA whose slice holds it.
             float *wx = D + (size_t) (t + x) * P + t;
             float *wy = D + (size_t) (t + y) * P + t;
-            if(Linear) {
-                // Row/column x get the new distances and row/column c-1 move
-                // into y; or, when x is c-1, the new distances go into y.
-                for(uint32_t i = ji; i < jhi; i += kThreads) {
-                    if(mv) {
-                        if(i == c - 1) continue;
-                        if(i == y) {
-                            __stcg(wy + y, __ldcg(r0 + (c - 1)));   // the last one's diagonal
-                            continue;
-                        }
-                        if(i == x) {
-                            __stcg(wx + x, ND[x]);
-                            const float nds = nd_src();
-                            __stcg(wx + y, nds);
-                            __stcg(wy + x, nds);
-                            continue;
-                        }
-                        const float nd = ND[i];
-                        __stcg(wx + i, nd);
-                        __stcg(D + (size_t) i * P + x, nd);
-                        const float v = i == ji ? v0 : __ldcg(r0 + i);
-                        __stcg(wy + i, v);
-                        __stcg(D + (size_t) i * P + y, v);
-                    } else {
-                        if(i == y || i == x) continue;
-                        const float nd = ND[i];
-                        __stcg(wy + i, nd);
-                        __stcg(D + (size_t) i * P + y, nd);
-                    }
-                }
-            } else
             for(uint32_t i = ji; i < jhi; i += kThreads) {
-                if(i == 0 || i == y) {
-                    if(i == y && y != 0) __stcg(wy + y, __ldcg(r0));   // logical 0's diagonal
+                if(Linear && !mv) {
+                    if(i == y || i == x) continue;
+                    const float nd = ND[i];
+                    __stcg(wy + i, nd);
+                    __stcg(D + (size_t) i * P + y, nd);
                     continue;
                 }
+                if(i == src || (!Linear && y == 0 && i == y)) continue;
+                if(i == y) {
+                    __stcg(wy + y, __ldcg(r0 + src));   // src's diagonal
+                    continue;
+                }
+                const float nd = ND[i];
                 if(i == x) {
-                    __stcg(wx + x, ND[x]);
-                    if(y != 0) {
-                        const float nds = nd_src();
+                    __stcg(wx + x, nd);
+                    if(mv) {
+                        unsigned r = 0;
+                        while(r + 1 < F && (uint64_t) c * (r + 1) / F <= src) ++r;
+                        const float nds = cluster.map_shared_rank(ND, r)[src];
                         __stcg(wx + y, nds);
                         __stcg(wy + x, nds);
                     }
                     continue;
                 }
-                const float nd = ND[i];
                 __stcg(wx + i, nd);
                 __stcg(D + (size_t) (t + i) * P + t + x, nd);
-                if(y != 0) {
+                if(mv) {
                     const float v = i == ji ? v0 : __ldcg(r0 + i);
                     __stcg(wy + i, v);
                     __stcg(D + (size_t) (t + i) * P + t + y, v);
