@@ -219,6 +219,7 @@ struct ScanView {
     float cm2, s_moved;
 };
 
+template <bool TailCut>
 __device__ __forceinline__ void scan_rows(const ScanView &v, uint32_t s, uint32_t ns, int warp, int lane,
                                           unsigned long long &best)
 {
@@ -229,11 +230,15 @@ __device__ __forceinline__ void scan_rows(const ScanView &v, uint32_t s, uint32_
     auto row_of = [&](uint32_t i) { return v.D + (size_t) (i == v.moved ? v.mslot : v.t + i) * v.P + base4; };
     // Q = (c-2) * D - S_i - S_j for the four cells of a chunk, two per packed
     // operation; cells at or past the row's end (column hi) get -inf.
-    auto chunk_q = [&](const float4 &d, uint32_t col, uint32_t hi, unsigned long long si2, float &q0, float &q1,
-                       float &q2, float &q3) {
+    auto chunk_raw = [&](const float4 &d, uint32_t col, unsigned long long si2, float &q0, float &q1, float &q2,
+                         float &q3) {
         const float4 s = *reinterpret_cast<const float4 *>(v.S + col);
         f2_split(sub2(sub2(mul2(cm2x2, f2(d.x, d.y)), si2), f2(s.x, s.y)), q0, q1);
         f2_split(sub2(sub2(mul2(cm2x2, f2(d.z, d.w)), si2), f2(s.z, s.w)), q2, q3);
+    };
+    auto chunk_q = [&](const float4 &d, uint32_t col, uint32_t hi, unsigned long long si2, float &q0, float &q1,
+                       float &q2, float &q3) {
+        chunk_raw(d, col, si2, q0, q1, q2, q3);
         if(col + 4 > hi) {
             if(col >= hi) q0 = -INFINITY;
             if(col + 1 >= hi) q1 = -INFINITY;
@@ -271,17 +276,40 @@ __device__ __forceinline__ void scan_rows(const ScanView &v, uint32_t s, uint32_
             const uint32_t nch = (hi - base4 + 3) >> 2;
             float bq = -INFINITY;
             uint32_t bg = 0;
+            // The row's last chunk, when it holds cells past the row's end:
+            // chunk nfull, in lane nfull % 32's slot (nfull % span) / 32 of
+            // the pass starting at g0 = tail_g0 (a pass spans 32 kBatch chunks).
+            constexpr uint32_t span = 32 * kBatch;
+            const uint32_t nfull = (hi - base4) >> 2, rem = (hi - base4) & 3u;
+            const uint32_t tail_g0 = (TailCut && rem && (nfull & 31u) == (uint32_t) lane)
+                                         ? nfull / span * span + (nfull & 31u)
+                                         : 0xffffffffu;
             for(uint32_t g0 = lane; g0 < nch; g0 += 32 * kBatch) {
                 float4 d[kBatch];
 #pragma unroll
                 for(int u = 0; u < kBatch; ++u)
                     if(g0 + 32 * u < nch) d[u] = __ldcg(reinterpret_cast<const float4 *>(row + 4 * (g0 + 32 * u)));
+                if(TailCut && g0 == tail_g0) {
+                    // D = -inf past the row's end gives Q = -inf there (NaN
+                    // when c = 2), which never wins.
+                    const uint32_t tu = (nfull % span) >> 5;
+#pragma unroll
+                    for(int u = 0; u < kBatch; ++u)
+                        if((uint32_t) u == tu) {
+                            d[u].w = -INFINITY;
+                            if(rem <= 2) d[u].z = -INFINITY;
+                            if(rem <= 1) d[u].y = -INFINITY;
+                        }
+                }
 #pragma unroll
                 for(int u = 0; u < kBatch; ++u) {
                     const uint32_t g = g0 + 32 * u;
                     if(g < nch) {
                         float q0, q1, q2, q3;
-                        chunk_q(d[u], base4 + 4 * g, hi, si2, q0, q1, q2, q3);
+                        if constexpr(TailCut)
+                            chunk_raw(d[u], base4 + 4 * g, si2, q0, q1, q2, q3);
+                        else
+                            chunk_q(d[u], base4 + 4 * g, hi, si2, q0, q1, q2, q3);
                         const float m = fmaxf(fmaxf(q0, q1), fmaxf(q2, q3));
                         if(m > bq) {
                             bq = m;
@@ -350,7 +378,8 @@ __device__ void nj_helper(const State &st, float *S, uint32_t hidx, uint32_t sid
     uint32_t c = n, t = 0, step = 0, pend = kNone, moved = kNone, mslot = 0;
     while(c > 1 && c > st.helper_c) {
         unsigned long long best = 0;
-        scan_rows(ScanView{st.D, S, P, t, c, pend, moved, mslot, (float) (c - 2), h_moved}, sidx, nscan, warp, lane,
+        scan_rows<!Linear>(ScanView{st.D, S, P, t, c, pend, moved, mslot, (float) (c - 2), h_moved}, sidx, nscan, warp,
+                           lane,
                   best);
         {
             const unsigned long long wm = warp_max(best);
@@ -497,7 +526,7 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             // This CTA's share of the rows of the logical lower triangle
             // (scan_rows), with +inf in S masking the dropped slots and those
             // of `moved` and the new node.
-            scan_rows(ScanView{D, S, P, t, c, pend, moved, mslot, cm2, s_moved_sh}, rank,
+            scan_rows<!Linear>(ScanView{D, S, P, t, c, pend, moved, mslot, cm2, s_moved_sh}, rank,
                       F + (helped ? st.helper_ctas : 0u), warp, lane, best);
         } else if(pend != kNone) {
             // The new node's row and column, from the distances the last join
@@ -687,6 +716,16 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             const uint32_t ji = jlo + tid;
             float a0 = ji < jhi ? __ldcg(rx + ji) : 0.0f, b0 = ji < jhi ? __ldcg(ry + ji) : 0.0f;
             const float v0 = (ji < jhi && mv) ? __ldcg(r0 + ji) : 0.0f;
+            // The thread of element x also writes src's new distance into
+            // D[x][y] and D[y][x], and the thread of element y src's diagonal
+            // into D[y][y]: their reads (none of those cells is written by
+            // this join) are issued here with the slice's, not after B.
+            float px = 0.0f, py = 0.0f;
+            if(mv && ji == x) {
+                px = __ldcg(rx + src);
+                py = __ldcg(ry + src);
+            }
+            if(mv && ji == y) px = __ldcg(r0 + src);
             auto s_of = [&](uint32_t i) { return i == moved ? s_moved : i == pend ? s_pend : S[t + i]; };
 
             // join_pair (sequential.cpp:247-267) on the slice. D[i][x] and
@@ -736,8 +775,8 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             // it was, and masks columns x and y): row and column x get the new
             // distances, and logical `src`'s row and column move into y (or,
             // in the linear order when x is the last, the new distances go
-            // into y). D[x][y] and D[y][x] take src's new distance, from the
-            // scanning CTA whose slice holds it.
+            // into y). D[x][y] and D[y][x] take src's new distance, which the
+            // thread of element x computes itself from its own reads.
             float *wx = D + (size_t) (t + x) * P + t;
             float *wy = D + (size_t) (t + y) * P + t;
             for(uint32_t i = ji; i < jhi; i += kThreads) {
@@ -750,16 +789,17 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
                 }
                 if(i == src || (!Linear && y == 0 && i == y)) continue;
                 if(i == y) {
-                    __stcg(wy + y, __ldcg(r0 + src));   // src's diagonal
+                    __stcg(wy + y, i == ji ? px : __ldcg(r0 + src));   // src's diagonal
                     continue;
                 }
                 const float nd = ND[i];
                 if(i == x) {
                     __stcg(wx + x, nd);
                     if(mv) {
-                        unsigned r = 0;
-                        while(r + 1 < F && (uint64_t) c * (r + 1) / F <= src) ++r;
-                        const float nds = cluster.map_shared_rank(ND, r)[src];
+                        // src's new distance, with the join's operations on
+                        // the same operands (read before B).
+                        const float ax = i == ji ? px : __ldcg(rx + src), ay = i == ji ? py : __ldcg(ry + src);
+                        const float nds = __double2float_rn(__dmul_rn((double) __fsub_rn(__fadd_rn(ax, ay), dxy), 0.5));
                         __stcg(wx + y, nds);
                         __stcg(wy + x, nds);
                     }
