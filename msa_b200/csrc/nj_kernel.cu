@@ -467,6 +467,10 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
     // Row sum of the new node `pend`, written here by CTA F after its fold,
     // while this CTA's S holds +inf in its slot (CTAs 0..F-1).
     __shared__ float s_pend_sh;
+    // A scanning CTA r's slice of the join, [c r / F, c (r + 1) / F), kept as
+    // quotients and remainders (q F + rem = c m for m = r and r + 1) that
+    // thread 0 steps down with c, so that no join divides.
+    __shared__ uint32_t sl_q[2], sl_rem[2];
 
     const unsigned K = cluster.num_blocks();
     const unsigned rank = cluster.block_rank();
@@ -490,6 +494,10 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
         s_moved_sh = 0.0f;
         s_pend_sh = 0.0f;
         hoff = 0;
+        for(int h = 0; h < 2; ++h) {
+            sl_q[h] = n * (rank + h) / F;
+            sl_rem[h] = n * (rank + h) % F;
+        }
     }
     unsigned long long t_last = clock64();
     auto mark = [&](int k) {
@@ -711,8 +719,7 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             // [c r / F, c (r + 1) / F), the slice it also writes back after B.
             // The loads of a thread's first element are issued here, and the
             // moved row's entry too, so the writes wait for no load.
-            const uint32_t jlo = (uint32_t) ((uint64_t) c * rank / F);
-            const uint32_t jhi = (uint32_t) ((uint64_t) c * (rank + 1) / F);
+            const uint32_t jlo = sl_q[0], jhi = sl_q[1];
             const uint32_t ji = jlo + tid;
             float a0 = ji < jhi ? __ldcg(rx + ji) : 0.0f, b0 = ji < jhi ? __ldcg(ry + ji) : 0.0f;
             const float v0 = (ji < jhi && mv) ? __ldcg(r0 + ji) : 0.0f;
@@ -813,6 +820,16 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
                     __stcg(D + (size_t) (t + i) * P + t + y, v);
                 }
             }
+            if(tid == 0)   // the slice of the next join, with c - 1 OTUs
+                for(int h = 0; h < 2; ++h) {
+                    const uint32_t m = rank + h;
+                    if(sl_rem[h] >= m) {
+                        sl_rem[h] -= m;
+                    } else {
+                        sl_rem[h] += F - m;
+                        --sl_q[h];
+                    }
+                }
             __syncthreads();   // the +inf masks above, before the scan
             if(timer) mark(4);
         }
