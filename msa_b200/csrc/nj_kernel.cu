@@ -469,7 +469,7 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
     __shared__ float s_pend_sh;
     // A scanning CTA r's slice of the join, [c r / F, c (r + 1) / F), kept as
     // quotients and remainders (q F + rem = c m for m = r and r + 1) that
-    // thread 0 steps down with c, so that no join divides.
+    // the CTA's last thread steps down with c, so that no join divides.
     __shared__ uint32_t sl_q[2], sl_rem[2];
 
     const unsigned K = cluster.num_blocks();
@@ -768,8 +768,10 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             // row the next scan reads. The new node's folded sum arrives in
             // s_pend_sh; the next join writes every slot but x's from the sums
             // it read, so a +inf slot ends up with its sum unless it is masked
-            // again.
-            if(tid == 0) {
+            // again. The CTA's last thread does it (and steps the slice down
+            // below): it holds no element of the slice (at most 854 at n <=
+            // 12800), so the threads that write wait for neither.
+            if(tid == kThreads - 1) {
                 if(mv) {
                     s_moved_sh = S[t + src];
                     S[t + y] = INFINITY;
@@ -820,7 +822,7 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
                     __stcg(D + (size_t) (t + i) * P + t + y, v);
                 }
             }
-            if(tid == 0)   // the slice of the next join, with c - 1 OTUs
+            if(tid == kThreads - 1)   // the slice of the next join, with c - 1 OTUs
                 for(int h = 0; h < 2; ++h) {
                     const uint32_t m = rank + h;
                     if(sl_rem[h] >= m) {
