@@ -323,14 +323,15 @@ __device__ __forceinline__ void scan_rows(const ScanView &v, uint32_t s, uint32_
         }
     }
     if(v.moved != kNone) {
-        const uint32_t rows = 2 * ((v.c - 1 + 2 * W - 1) / (2 * W));
         for(uint32_t r = (uint32_t) lane;;) {
             if(mi) {
                 const float q = __fsub_rn(__fsub_rn(__fmul_rn(v.cm2, mq), v.S[v.t + mi]), s_moved);
                 best = umax64(best, pack(order_key(q), mi, v.moved));
             }
             r += 32;
-            if(r >= rows) break;
+            // The warp has 2 ceil((c-1) / 2W) places: r is past them once its
+            // block of 2W places starts at or after row c-1's place count.
+            if((r >> 1) * 2 * W >= v.c - 1) break;
             mi = moved_row(r);
             if(mi) mq = __ldcg(v.D + (size_t) (v.t + mi) * v.P + v.mslot);
         }
