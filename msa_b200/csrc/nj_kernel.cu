@@ -770,8 +770,9 @@ __global__ void __launch_bounds__(kThreads, 1) nj_cluster_kernel(State st)
             // s_pend_sh; the next join writes every slot but x's from the sums
             // it read, so a +inf slot ends up with its sum unless it is masked
             // again. The CTA's last thread does it (and steps the slice down
-            // below): it holds no element of the slice (at most 854 at n <=
-            // 12800), so the threads that write wait for neither.
+            // below): in a 16-CTA cluster it holds no element of the slice
+            // (at most 854 at n <= 12800), so the threads that write wait for
+            // neither (with fewer CTAs it may also write, after the masks).
             if(tid == kThreads - 1) {
                 if(mv) {
                     s_moved_sh = S[t + src];
